@@ -1,0 +1,112 @@
+/* rsx: the soccar 1v1 8-tick decision step on B200 (sm_100a), as a C ABI.
+ *
+ * Drop-in for the device path of the reference's Rust host crate (crates/rocketsim-cuda/src/device.rs, SimDevice):
+ * arena states in AoSoA-32 buffers of u32 words (word w of arena a at (a/32)*32*2784 + w*32 + a%32), one StaticData
+ * of 317,895 words per car pairing, controls as 8 words per car, one result word per arena.  Every entry point returns
+ * an int status (RSX_OK or a negative RSX_E*); nothing throws across the ABI.  Launch entry points are asynchronous on
+ * the handle's stream; downloads synchronise.  All layouts are the reference's (cuda/sim/arena_state.cuh:42-339).
+ */
+#ifndef RSX_H
+#define RSX_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define RSX_OK 0
+#define RSX_E_ARG (-1)      /* a bad argument (null handle, block outside 1..64, buffer too short) */
+#define RSX_E_CUDA (-2)     /* a CUDA runtime error (rsx_last_error() names it) */
+#define RSX_E_NODEV (-3)    /* no CUDA device / no sm_100 device */
+#define RSX_E_TIMEOUT (-4)  /* a bounded device wait gave up (persistent kernel) */
+
+/* ---- constants (device.rs:16-28, arena_step.cuh:16-18) ---- */
+#define RSX_TICKS_PER_DECISION 8u
+#define RSX_SCORED_MASK 0xFFu
+#define RSX_UNIMPLEMENTED 0x80000000u
+#define RSX_OVERFLOW 0x40000000u
+#define RSX_SIM8_BLOCK 32u
+#define RSX_MAX_BLOCK 64u
+
+/* Controls of one car (arena_state.cuh:77-80): throttle, steer, pitch, yaw, roll as f32, then jump, boost, handbrake 0/1. */
+typedef struct rsx_controls {
+  float throttle, steer, pitch, yaw, roll;
+  uint32_t jump, boost, handbrake;
+} rsx_controls;
+
+typedef struct rsx_device rsx_device;    /* SimDevice: a device, its stream */
+typedef struct rsx_static rsx_static;    /* DeviceStatic: one or more StaticData on the device */
+typedef struct rsx_states rsx_states;    /* DeviceStates: n arenas in one AoSoA-32 buffer */
+
+/* ---- layout (layout.rs; lf_arena_words / lf_tick_words / lf_static_words of csrc/phase.cpp:18-22) ---- */
+uint64_t rsx_arena_words(void);            /* 2784 */
+uint64_t rsx_tick_words(void);             /* 2567: the words that cross a tick */
+uint64_t rsx_static_words(void);           /* 317,895 */
+uint64_t rsx_aosoa_words(uint32_t n);      /* words of an AoSoA-32 buffer of n arenas (aosoa.cuh:15) */
+uint64_t rsx_aosoa_index(uint32_t a, uint32_t w);  /* aosoa.cuh:17 */
+/* host-side pack / unpack between n contiguous ArenaStates and AoSoA-32 (aosoa.rs:9-38) */
+void rsx_aosoa_pack(const uint32_t* states, uint32_t n, uint32_t* aosoa);
+void rsx_aosoa_unpack(const uint32_t* aosoa, uint32_t n, uint32_t* states);
+const char* rsx_last_error(void);
+
+/* ---- device (SimDevice::new, device.rs:53-67; cuda.rs:18-28 context with an 8 KiB stack) ---- */
+int rsx_device_create(int ordinal, rsx_device** out);
+int rsx_device_destroy(rsx_device* dev);
+int rsx_sync(rsx_device* dev);
+void* rsx_device_stream(rsx_device* dev);  /* the handle's cudaStream_t */
+
+/* ---- static data (SimDevice::upload_static, device.rs:69) ---- */
+/* `count` StaticData back to back (count 1 is the reference's single car pairing) */
+int rsx_static_upload(rsx_device* dev, const uint32_t* words, uint32_t count, rsx_static** out);
+int rsx_static_free(rsx_static* sd);
+const void* rsx_static_device_ptr(rsx_static* sd);
+
+/* ---- states (upload_states / alloc_states / download_words, device.rs:74-90) ---- */
+int rsx_states_alloc(rsx_device* dev, uint32_t n, rsx_states** out);
+int rsx_states_free(rsx_states* st);
+int rsx_states_upload(rsx_device* dev, rsx_states* st, const uint32_t* aosoa);     /* rsx_aosoa_words(n) words */
+int rsx_states_download(rsx_device* dev, rsx_states* st, uint32_t* aosoa);         /* synchronises */
+uint32_t* rsx_states_device_ptr(rsx_states* st);
+
+/* ---- the decision (SimDevice::sim8, device.rs:155-168; kernel sim.cu:95-104) ----
+ * One decision of every arena in place: 8 ticks with controls[a*2+i] (device memory, 16 words per arena), result[a] the
+ * scored tick | RSX_UNIMPLEMENTED | RSX_OVERFLOW (device memory).  block: 1..64 threads (RSX_SIM8_BLOCK in production).
+ * trace: null, or 8 AoSoA buffers (8 * rsx_aosoa_words(n) words, device memory) that receive the state after each tick. */
+int rsx_sim8(rsx_device* dev, rsx_states* st, rsx_static* sd, const rsx_controls* d_controls, uint32_t* d_result, uint32_t block,
+             uint32_t* d_trace);
+/* the same on raw device pointers and a caller stream (the path torch / CUDA-graph callers use) */
+int rsx_sim8_raw(uint32_t* d_states, uint32_t n, const void* d_static, const rsx_controls* d_controls, uint32_t* d_result,
+                 uint32_t block, uint32_t* d_trace, void* stream);
+/* one full tick (step_tick_k, sim.cu:46-53) and one phase (phase_k, sim.cu:27-34); status[a] is the PhaseStatus */
+int rsx_step_tick(rsx_device* dev, rsx_states* st, rsx_static* sd, int32_t* d_status);
+int rsx_phase(rsx_device* dev, int k, rsx_states* st, rsx_static* sd, int32_t* d_status);
+/* the copy-in / copy-out round trip (sim_identity[_tick], sim.cu:9-24) */
+int rsx_identity(rsx_device* dev, const uint32_t* d_in, uint32_t* d_out, uint32_t n, int tick_only);
+
+/* ---- extensions (no counterpart in the reference's kernel set; the functions above are unchanged by them) ----
+ * Per-arena car pairing: d_static points at `count` StaticData, sd_index[a] (u8, device memory) selects arena a's. */
+int rsx_sim8_multi_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                       const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, uint32_t block, void* stream);
+/* The persistent kernel: `grid` resident blocks pull work items (`granularity` arenas) from device queues; with
+ * d_bins non-null, arenas are taken bin by bin (bins from rsx_bin_arenas), so warps step arenas of like cost.
+ * Results do not depend on grid, block, granularity or binning (no cross-arena arithmetic). */
+int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                            const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or,
+                            const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid, uint32_t block,
+                            uint32_t granularity, void* stream);
+
+/* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
+/* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */
+int rsx_build_static(uint32_t* words, uint64_t seed, int preset0, int preset1);
+/* n fresh ArenaStates (2784 words each, contiguous): scenario mix[5] = kickoff, open play, head-on, pinch, pad contention */
+int rsx_make_states(const uint32_t* static_words, uint32_t* states, uint32_t n, uint64_t seed, const float* mix);
+/* the same source compiled for the host (for debugging and CPU-side checks; the device entry points never call these) */
+int rsx_host_phase(int k, uint32_t* state_words, const uint32_t* static_words);
+uint32_t rsx_host_decide(uint32_t* state_words, const uint32_t* static_words, const rsx_controls* controls2);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,248 @@
+"""Python host side of the soccar decision step: a ctypes mirror of the reference's Rust host crate API
+(crates/rocketsim-cuda/src/device.rs SimDevice: new, upload_static, upload_states, alloc_states, download_states,
+upload_controls, sim8, step_tick, phase, identity) over the C ABI of librsx.so (include/rsx.h).
+
+Device memory for controls / results comes from torch (plumbing only); states and static data are owned by the
+library's handles.  Nothing here computes physics: every step runs the CUDA kernels, and a missing library is an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librsx.so")
+
+ARENA_WORDS = 2784
+TICK_WORDS = 2567
+STATIC_WORDS = 317895
+TICKS_PER_DECISION = 8
+SCORED_MASK = 0xFF
+UNIMPLEMENTED = 0x80000000
+OVERFLOW = 0x40000000
+SIM8_BLOCK = 32
+MAX_BLOCK = 64
+NUM_CARS = 2
+CONTROL_WORDS = 8
+
+# offsets of a few words of ArenaState (the reference's layout)
+W_EVENTS = TICK_WORDS - 1
+MIX_HEADLINE = (0.20, 0.50, 0.15, 0.10, 0.05)  # kickoff, open play, head-on, pinch, pad contention
+MIX_KICKOFF = (1.0, 0.0, 0.0, 0.0, 0.0)
+MIX_CONTACT_HEAVY = (0.10, 0.20, 0.30, 0.40, 0.0)
+
+_lib = None
+
+
+class RsxError(RuntimeError):
+    pass
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RsxError(f"librsx.so is not built ({LIB_PATH}); run `make -C rocketsim-cuda_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.rsx_arena_words.restype = ctypes.c_uint64
+        L.rsx_tick_words.restype = ctypes.c_uint64
+        L.rsx_static_words.restype = ctypes.c_uint64
+        L.rsx_aosoa_words.restype = ctypes.c_uint64
+        L.rsx_aosoa_words.argtypes = [ctypes.c_uint32]
+        L.rsx_aosoa_index.restype = ctypes.c_uint64
+        L.rsx_aosoa_index.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.rsx_aosoa_pack.argtypes = [u32p, ctypes.c_uint32, u32p]
+        L.rsx_aosoa_unpack.argtypes = [u32p, ctypes.c_uint32, u32p]
+        L.rsx_last_error.restype = ctypes.c_char_p
+        L.rsx_build_static.argtypes = [u32p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+        L.rsx_make_states.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
+        L.rsx_host_phase.argtypes = [ctypes.c_int, u32p, u32p]
+        L.rsx_host_decide.argtypes = [u32p, u32p, u32p]
+        L.rsx_host_decide.restype = ctypes.c_uint32
+        vp = ctypes.c_void_p
+        L.rsx_device_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.rsx_device_destroy.argtypes = [vp]
+        L.rsx_sync.argtypes = [vp]
+        L.rsx_device_stream.argtypes = [vp]
+        L.rsx_device_stream.restype = vp
+        L.rsx_static_upload.argtypes = [vp, u32p, ctypes.c_uint32, ctypes.POINTER(vp)]
+        L.rsx_static_free.argtypes = [vp]
+        L.rsx_static_device_ptr.argtypes = [vp]
+        L.rsx_static_device_ptr.restype = vp
+        L.rsx_states_alloc.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(vp)]
+        L.rsx_states_free.argtypes = [vp]
+        L.rsx_states_upload.argtypes = [vp, vp, u32p]
+        L.rsx_states_download.argtypes = [vp, vp, u32p]
+        L.rsx_states_device_ptr.argtypes = [vp]
+        L.rsx_states_device_ptr.restype = vp
+        L.rsx_sim8.argtypes = [vp, vp, vp, vp, vp, ctypes.c_uint32, vp]
+        L.rsx_sim8_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint32, vp, vp]
+        L.rsx_step_tick.argtypes = [vp, vp, vp, vp]
+        L.rsx_phase.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        L.rsx_identity.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_int]
+        L.rsx_sim8_multi_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]
+        L.rsx_sim8_persistent_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_uint32, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def check(rc: int, what: str) -> None:
+    if rc < 0:
+        raise RsxError(f"{what} failed ({rc}): {lib().rsx_last_error().decode(errors='replace')}")
+
+
+# ---- host-side data ----------------------------------------------------------------------------------------------
+def build_static(seed: int = 7, preset0: int = 0, preset1: int = 0) -> np.ndarray:
+    """One StaticData of the synthetic soccar world for the car pairing (preset0, preset1)."""
+    sd = np.zeros(STATIC_WORDS, np.uint32)
+    check(lib().rsx_build_static(_p(sd), seed, preset0, preset1), "rsx_build_static")
+    return sd
+
+
+def make_states(sd: np.ndarray, n: int, seed: int, mix: Sequence[float] = MIX_HEADLINE) -> np.ndarray:
+    """n seeded start states (n x 2784 words)."""
+    st = np.zeros((n, ARENA_WORDS), np.uint32)
+    m = (ctypes.c_float * 5)(*mix)
+    check(lib().rsx_make_states(_p(sd), _p(st), n, seed, m), "rsx_make_states")
+    return st
+
+
+def aosoa_words(n: int) -> int:
+    return int(lib().rsx_aosoa_words(n))
+
+
+def pack(states: np.ndarray) -> np.ndarray:
+    """n x 2784 ArenaStates -> AoSoA-32 words (numpy, vectorised: the layout of aosoa.cuh:17)."""
+    n = states.shape[0]
+    blocks = (n + 31) // 32
+    pad = np.zeros((blocks * 32, ARENA_WORDS), np.uint32)
+    pad[:n] = states
+    return np.ascontiguousarray(pad.reshape(blocks, 32, ARENA_WORDS).transpose(0, 2, 1)).reshape(-1)
+
+
+def unpack(words: np.ndarray, n: int) -> np.ndarray:
+    blocks = (n + 31) // 32
+    return np.ascontiguousarray(words.reshape(blocks, ARENA_WORDS, 32).transpose(0, 2, 1)).reshape(blocks * 32, ARENA_WORDS)[:n]
+
+
+def random_controls(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Controls[n][2] as words: each axis uniform in {-1, 0, 1}, jump / boost / handbrake Bernoulli(0.5)."""
+    c = np.zeros((n, NUM_CARS, CONTROL_WORDS), np.uint32)
+    axes = rng.integers(-1, 2, size=(n, NUM_CARS, 5)).astype(np.float32)
+    c[:, :, :5] = axes.view(np.uint32)
+    c[:, :, 5:] = rng.integers(0, 2, size=(n, NUM_CARS, 3)).astype(np.uint32)
+    return c.reshape(n, NUM_CARS * CONTROL_WORDS)
+
+
+# ---- the device handle (SimDevice) --------------------------------------------------------------------------------
+class SimDevice:
+    def __init__(self, ordinal: int = 0):
+        import torch  # device memory for controls and results
+
+        self.torch = torch
+        h = ctypes.c_void_p()
+        check(lib().rsx_device_create(ordinal, ctypes.byref(h)), "rsx_device_create")
+        self.h = h
+        self.ordinal = ordinal
+        self.device = torch.device("cuda", ordinal)
+
+    def close(self):
+        if self.h:
+            lib().rsx_device_destroy(self.h)
+            self.h = None
+
+    def stream_ptr(self) -> int:
+        return lib().rsx_device_stream(self.h)
+
+    def upload_static(self, sds: np.ndarray) -> "DeviceStatic":
+        sds = np.ascontiguousarray(sds.reshape(-1, STATIC_WORDS), dtype=np.uint32)
+        h = ctypes.c_void_p()
+        check(lib().rsx_static_upload(self.h, _p(sds.reshape(-1)), sds.shape[0], ctypes.byref(h)), "rsx_static_upload")
+        return DeviceStatic(h, sds.shape[0])
+
+    def alloc_states(self, n: int) -> "DeviceStates":
+        h = ctypes.c_void_p()
+        check(lib().rsx_states_alloc(self.h, n, ctypes.byref(h)), "rsx_states_alloc")
+        return DeviceStates(h, n)
+
+    def upload_states(self, states: np.ndarray) -> "DeviceStates":
+        d = self.alloc_states(states.shape[0])
+        words = pack(states)
+        check(lib().rsx_states_upload(self.h, d.h, _p(words)), "rsx_states_upload")
+        return d
+
+    def download_words(self, d: "DeviceStates") -> np.ndarray:
+        out = np.zeros(aosoa_words(d.n), np.uint32)
+        check(lib().rsx_states_download(self.h, d.h, _p(out)), "rsx_states_download")
+        return out
+
+    def download_states(self, d: "DeviceStates") -> np.ndarray:
+        return unpack(self.download_words(d), d.n)
+
+    def upload_controls(self, controls: np.ndarray):
+        t = self.torch.from_numpy(np.ascontiguousarray(controls.view(np.int32))).to(self.device)
+        return t
+
+    def alloc_result(self, n: int):
+        return self.torch.zeros(n, dtype=self.torch.int32, device=self.device)
+
+    def sim8(self, states: "DeviceStates", sd: "DeviceStatic", controls, result, block: int = SIM8_BLOCK, trace=None) -> None:
+        if not (1 <= block <= MAX_BLOCK):
+            raise ValueError(f"sim8: block of {block} threads")
+        if controls.numel() < states.n * 16 or result.numel() < states.n:
+            raise ValueError("sim8: buffers too short")
+        tp = trace.data_ptr() if trace is not None else None
+        check(lib().rsx_sim8(self.h, states.h, sd.h, controls.data_ptr(), result.data_ptr(), block, tp), "rsx_sim8")
+
+    def step_tick(self, states: "DeviceStates", sd: "DeviceStatic") -> np.ndarray:
+        status = self.torch.zeros(states.n, dtype=self.torch.int32, device=self.device)
+        check(lib().rsx_step_tick(self.h, states.h, sd.h, status.data_ptr()), "rsx_step_tick")
+        self.sync()
+        return status.cpu().numpy()
+
+    def phase(self, k: int, states: "DeviceStates", sd: "DeviceStatic") -> np.ndarray:
+        status = self.torch.zeros(states.n, dtype=self.torch.int32, device=self.device)
+        check(lib().rsx_phase(self.h, k, states.h, sd.h, status.data_ptr()), "rsx_phase")
+        self.sync()
+        return status.cpu().numpy()
+
+    def sync(self) -> None:
+        check(lib().rsx_sync(self.h), "rsx_sync")
+
+
+class DeviceStatic:
+    def __init__(self, h, count):
+        self.h = h
+        self.count = count
+
+    def ptr(self) -> int:
+        return lib().rsx_static_device_ptr(self.h)
+
+    def free(self):
+        if self.h:
+            lib().rsx_static_free(self.h)
+            self.h = None
+
+
+class DeviceStates:
+    def __init__(self, h, n):
+        self.h = h
+        self.n = n
+
+    def ptr(self) -> int:
+        return lib().rsx_states_device_ptr(self.h)
+
+    def free(self):
+        if self.h:
+            lib().rsx_states_free(self.h)
+            self.h = None
