@@ -102,9 +102,20 @@ int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_static
 int rsx_build_static(uint32_t* words, uint64_t seed, int preset0, int preset1);
 /* n fresh ArenaStates (2784 words each, contiguous): scenario mix[5] = kickoff, open play, head-on, pinch, pad contention */
 int rsx_make_states(const uint32_t* static_words, uint32_t* states, uint32_t n, uint64_t seed, const float* mix);
+/* per-arena car pairings: statics[count], sd_index[a] < count selects arena a's StaticData */
+int rsx_make_states_multi(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, uint32_t* states, uint32_t n,
+                          uint64_t seed, const float* mix);
 /* the same source compiled for the host (for debugging and CPU-side checks; the device entry points never call these) */
 int rsx_host_phase(int k, uint32_t* state_words, const uint32_t* static_words);
 uint32_t rsx_host_decide(uint32_t* state_words, const uint32_t* static_words, const rsx_controls* controls2);
+
+/* ---- verification of the FP64-free correctly rounded libm (sin, cos, tan, atan2, pow and the auto-flip helpers) ----
+ * fn 0 sin, 1 cos, 2 tan, 3 atan2(a, b), 4 pow(a, b), 5 float(double atan2(a, b)), 6 float(double hypot(a, b)) */
+int rsx_libm_host(int fn, const float* a, const float* b, float* out, uint64_t n);
+/* order-independent hash of f over [first_bits, first_bits + count): sum of mix64((x << 32) | f(x)), NaN canonical */
+uint64_t rsx_libm_hash_host(int fn, uint32_t first_bits, uint32_t count);
+/* the same hash on the device for chunks of 2^24 inputs (fn 0..2), d_hashes[nchunks] */
+int rsx_libm_chunk_hashes(int fn, uint32_t first_chunk, uint32_t nchunks, uint64_t* d_hashes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,223 @@
+// The device entry points of the C ABI (include/rsx.h): the handles (device + stream, static data, states), uploads and
+// downloads, and the launches of the decision kernels (kern_*.cu).  Status codes, never exceptions, cross the ABI.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <mutex>
+#include "../../include/rsx.h"
+#include "state.cuh"
+
+using namespace rsx;
+
+cudaError_t rsx_launch_sim8(uint32_t* states, const void* sd, const void* controls, uint32_t* result, uint32_t n, uint32_t* trace,
+                            uint32_t block, cudaStream_t s);
+cudaError_t rsx_launch_sim8_multi(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result,
+                                  uint32_t* ev_or, uint32_t n, uint32_t block, cudaStream_t s);
+cudaError_t rsx_launch_sim8_persistent(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result,
+                                       uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t gran, uint32_t grid,
+                                       uint32_t block, cudaStream_t s);
+cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
+cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
+cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
+
+
+struct rsx_device {
+  int ordinal;
+  cudaStream_t stream;
+};
+struct rsx_static {
+  rsx_device* dev;
+  void* d;
+  uint32_t count;
+};
+struct rsx_states {
+  rsx_device* dev;
+  uint32_t* d;
+  uint32_t n;
+};
+
+static thread_local char g_err[256] = "";
+static int fail(cudaError_t e, const char* where) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+  return RSX_E_CUDA;
+}
+#define RSX_CK(x)                          \
+  do {                                     \
+    cudaError_t e_ = (x);                  \
+    if (e_ != cudaSuccess) return fail(e_, #x); \
+  } while (0)
+
+static int configure_current(void) {
+  static std::once_flag once[64];
+  int dev = 0;
+  RSX_CK(cudaGetDevice(&dev));
+  static int status[64];
+  std::call_once(once[dev & 63], [&] {
+    // the phases run as calls with large frames (the solver's rows, the narrowphase jobs): reserve the stack they need
+    size_t want = 32 * 1024;
+    cudaError_t e = cudaDeviceSetLimit(cudaLimitStackSize, want);
+    status[dev & 63] = e == cudaSuccess ? RSX_OK : fail(e, "cudaDeviceSetLimit(stack)");
+  });
+  return status[dev & 63];
+}
+
+extern "C" {
+
+const char* rsx_last_error(void) { return g_err; }
+
+int rsx_device_create(int ordinal, rsx_device** out) {
+  if (!out) return RSX_E_ARG;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0 || ordinal < 0 || ordinal >= count) {
+    snprintf(g_err, sizeof(g_err), "no CUDA device %d", ordinal);
+    return RSX_E_NODEV;
+  }
+  cudaDeviceProp p;
+  RSX_CK(cudaGetDeviceProperties(&p, ordinal));
+  if (p.major != 10) {
+    snprintf(g_err, sizeof(g_err), "device %d is sm_%d%d; this library is built for sm_100a", ordinal, p.major, p.minor);
+    return RSX_E_NODEV;
+  }
+  RSX_CK(cudaSetDevice(ordinal));
+  int c = configure_current();
+  if (c != RSX_OK) return c;
+  rsx_device* d = new rsx_device;
+  d->ordinal = ordinal;
+  cudaError_t e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete d;
+    return fail(e, "cudaStreamCreate");
+  }
+  *out = d;
+  return RSX_OK;
+}
+
+int rsx_device_destroy(rsx_device* dev) {
+  if (!dev) return RSX_E_ARG;
+  cudaStreamSynchronize(dev->stream);
+  cudaStreamDestroy(dev->stream);
+  delete dev;
+  return RSX_OK;
+}
+
+int rsx_sync(rsx_device* dev) {
+  if (!dev) return RSX_E_ARG;
+  RSX_CK(cudaStreamSynchronize(dev->stream));
+  return RSX_OK;
+}
+
+void* rsx_device_stream(rsx_device* dev) { return dev ? (void*)dev->stream : nullptr; }
+
+int rsx_static_upload(rsx_device* dev, const uint32_t* words, uint32_t count, rsx_static** out) {
+  if (!dev || !words || !out || count == 0) return RSX_E_ARG;
+  RSX_CK(cudaSetDevice(dev->ordinal));
+  size_t bytes = sizeof(StaticData) * (size_t)count;
+  void* d = nullptr;
+  RSX_CK(cudaMalloc(&d, bytes));
+  cudaError_t e = cudaMemcpyAsync(d, words, bytes, cudaMemcpyHostToDevice, dev->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(dev->stream);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(e, "static upload");
+  }
+  *out = new rsx_static{dev, d, count};
+  return RSX_OK;
+}
+int rsx_static_free(rsx_static* sd) {
+  if (!sd) return RSX_E_ARG;
+  cudaFree(sd->d);
+  delete sd;
+  return RSX_OK;
+}
+const void* rsx_static_device_ptr(rsx_static* sd) { return sd ? sd->d : nullptr; }
+
+int rsx_states_alloc(rsx_device* dev, uint32_t n, rsx_states** out) {
+  if (!dev || !out || n == 0) return RSX_E_ARG;
+  RSX_CK(cudaSetDevice(dev->ordinal));
+  uint32_t* d = nullptr;
+  RSX_CK(cudaMalloc(&d, aosoa_words(n) * 4));
+  RSX_CK(cudaMemsetAsync(d, 0, aosoa_words(n) * 4, dev->stream));
+  *out = new rsx_states{dev, d, n};
+  return RSX_OK;
+}
+int rsx_states_free(rsx_states* st) {
+  if (!st) return RSX_E_ARG;
+  cudaFree(st->d);
+  delete st;
+  return RSX_OK;
+}
+int rsx_states_upload(rsx_device* dev, rsx_states* st, const uint32_t* aosoa) {
+  if (!dev || !st || !aosoa) return RSX_E_ARG;
+  RSX_CK(cudaMemcpyAsync(st->d, aosoa, aosoa_words(st->n) * 4, cudaMemcpyHostToDevice, dev->stream));
+  RSX_CK(cudaStreamSynchronize(dev->stream));
+  return RSX_OK;
+}
+int rsx_states_download(rsx_device* dev, rsx_states* st, uint32_t* aosoa) {
+  if (!dev || !st || !aosoa) return RSX_E_ARG;
+  RSX_CK(cudaMemcpyAsync(aosoa, st->d, aosoa_words(st->n) * 4, cudaMemcpyDeviceToHost, dev->stream));
+  RSX_CK(cudaStreamSynchronize(dev->stream));
+  return RSX_OK;
+}
+uint32_t* rsx_states_device_ptr(rsx_states* st) { return st ? st->d : nullptr; }
+
+int rsx_sim8_raw(uint32_t* d_states, uint32_t n, const void* d_static, const rsx_controls* d_controls, uint32_t* d_result, uint32_t block,
+                 uint32_t* d_trace, void* stream) {
+  if (!d_states || !d_static || !d_controls || !d_result || block < 1 || block > RSX_MAX_BLOCK) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  int c = configure_current();
+  if (c != RSX_OK) return c;
+  RSX_CK(rsx_launch_sim8(d_states, d_static, d_controls, d_result, n, d_trace, block, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_sim8(rsx_device* dev, rsx_states* st, rsx_static* sd, const rsx_controls* d_controls, uint32_t* d_result, uint32_t block,
+             uint32_t* d_trace) {
+  if (!dev || !st || !sd) return RSX_E_ARG;
+  return rsx_sim8_raw(st->d, st->n, sd->d, d_controls, d_result, block, d_trace, dev->stream);
+}
+
+int rsx_step_tick(rsx_device* dev, rsx_states* st, rsx_static* sd, int32_t* d_status) {
+  if (!dev || !st || !sd || !d_status) return RSX_E_ARG;
+  RSX_CK(rsx_launch_step_tick(st->d, sd->d, st->n, d_status, dev->stream));
+  return RSX_OK;
+}
+
+int rsx_phase(rsx_device* dev, int k, rsx_states* st, rsx_static* sd, int32_t* d_status) {
+  if (!dev || !st || !sd || !d_status || k < 0 || k >= 10) return RSX_E_ARG;
+  RSX_CK(rsx_launch_phase(k, st->d, sd->d, st->n, d_status, dev->stream));
+  return RSX_OK;
+}
+
+int rsx_identity(rsx_device* dev, const uint32_t* d_in, uint32_t* d_out, uint32_t n, int tick_only) {
+  if (!dev || !d_in || !d_out) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_identity(d_in, d_out, n, tick_only, dev->stream));
+  return RSX_OK;
+}
+
+int rsx_sim8_multi_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                       uint32_t* d_result, uint32_t* d_event_or, uint32_t block, void* stream) {
+  if (!d_states || !d_statics || !d_controls || !d_result || block < 1 || block > RSX_MAX_BLOCK) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  int c = configure_current();
+  if (c != RSX_OK) return c;
+  RSX_CK(rsx_launch_sim8_multi(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, n, block, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                            uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
+                            uint32_t block, uint32_t granularity, void* stream) {
+  if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_MAX_BLOCK || (block & 31) ||
+      grid == 0 || granularity == 0)
+    return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  int c = configure_current();
+  if (c != RSX_OK) return c;
+  RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, (cudaStream_t)stream));
+  RSX_CK(rsx_launch_sim8_persistent(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
+                                    granularity, grid, block, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+}  // extern "C"

@@ -453,7 +453,7 @@ RSX_F float powf_cr(float x, float y) {
   U128 tm = umulq(Lm, small(my, 124 - 23));  // |t| = tm * 2^(Le + ey)
   int te = Le + ey;
   // normalise tm to [1, 2) * 2^te
-  if (is_zero(tm)) return from_bits(0x3F800000u | 0u);
+  if (is_zero(tm)) return from_bits(0x3F800000u | rsign);  // |x| == 1: (+-1)^y
   int lead = 127 - clz(tm);
   te += lead - 124;
   tm = lead > 124 ? shr(tm, lead - 124) : shl(tm, 124 - lead);

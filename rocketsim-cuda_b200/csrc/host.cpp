@@ -10,6 +10,7 @@ namespace rsx {
 namespace world {
 int build_static(StaticData* sd, uint64_t seed, int preset0, int preset1);
 void make_states(const StaticData& sd, ArenaState* out, uint32_t n, uint64_t seed, const float* mix);
+void make_states_multi(const StaticData* sds, const uint8_t* idx, ArenaState* out, uint32_t n, uint64_t seed, const float* mix);
 }  // namespace world
 }  // namespace rsx
 
@@ -42,6 +43,15 @@ int rsx_build_static(uint32_t* words, uint64_t seed, int preset0, int preset1) {
 int rsx_make_states(const uint32_t* static_words, uint32_t* states, uint32_t n, uint64_t seed, const float* mix) {
   if (!static_words || !states || !mix) return RSX_E_ARG;
   world::make_states(*reinterpret_cast<const StaticData*>(static_words), reinterpret_cast<ArenaState*>(states), n, seed, mix);
+  return RSX_OK;
+}
+
+int rsx_make_states_multi(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, uint32_t* states, uint32_t n, uint64_t seed,
+                          const float* mix) {
+  if (!statics || !sd_index || !states || !mix) return RSX_E_ARG;
+  for (uint32_t a = 0; a < n; ++a)
+    if (sd_index[a] >= count) return RSX_E_ARG;
+  world::make_states_multi(reinterpret_cast<const StaticData*>(statics), sd_index, reinterpret_cast<ArenaState*>(states), n, seed, mix);
   return RSX_OK;
 }
 

@@ -1,0 +1,34 @@
+// The persistent decision kernel: `gridDim.x` resident blocks, each warp repeatedly claiming 32 * `gran` consecutive
+// entries of `order` (arena indices; identity when null) with one atomicAdd on a device counter.  With a binned order
+// (arenas sorted by predicted contact cost), the lanes of a warp step arenas of like cost.  Nothing waits on another
+// block: a claim past n ends the warp.  The counter must be zero at launch.
+#include "kern_common.cuh"
+
+extern "C" __global__ void __launch_bounds__(kMaxBlock, 1) k_sim8_persistent(uint32_t* states, const StaticData* sds, const uint8_t* sd_index,
+                                                                             const Controls* controls, uint32_t* result, uint32_t* ev_or,
+                                                                             const uint32_t* order, uint32_t* counter, uint32_t n,
+                                                                             uint32_t gran) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u * gran);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= n) break;
+    for (uint32_t g = 0; g < gran; ++g) {
+      uint32_t i = base + g * 32u + lane;
+      if (i < n) {
+        uint32_t a = order ? order[i] : i;
+        const StaticData& D = sds[sd_index ? sd_index[a] : 0];
+        result[a] = decide_arena(states, D, controls, a, nullptr, 0, ev_or);
+      }
+    }
+  }
+}
+
+cudaError_t rsx_launch_sim8_persistent(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result,
+                                       uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t gran, uint32_t grid,
+                                       uint32_t block, cudaStream_t s) {
+  k_sim8_persistent<<<grid, block, 0, s>>>(states, (const StaticData*)sds, sd_index, (const Controls*)controls, result, ev_or, order, counter, n,
+                                           gran);
+  return cudaGetLastError();
+}

@@ -611,12 +611,21 @@ static void init_car(ArenaState& s, const StaticData& sd, int ci, const CarPose&
   sim::set_body_pose(b, sd.bodies[sd.cars[ci].body], Aff{p.rot, p.pos * BT}, p.vel * BT, p.ang);
 }
 
+// arena a's start state: a function of (seed, a) and its StaticData only
+static void make_state(const StaticData& sd, ArenaState& s, uint32_t a, uint64_t seed, const float* mix);
+
 void make_states(const StaticData& sd, ArenaState* out, uint32_t n, uint64_t seed, const float* mix) {
+  for (uint32_t a = 0; a < n; ++a) make_state(sd, out[a], a, seed, mix);
+}
+void make_states_multi(const StaticData* sds, const uint8_t* idx, ArenaState* out, uint32_t n, uint64_t seed, const float* mix) {
+  for (uint32_t a = 0; a < n; ++a) make_state(sds[idx[a]], out[a], a, seed, mix);
+}
+
+static void make_state(const StaticData& sd, ArenaState& s, uint32_t a, uint64_t seed, const float* mix) {
   const float HXF = 4096.0f - 200.0f, HYF = 5120.0f - 250.0f;
-  for (uint32_t a = 0; a < n; ++a) {
+  {
     Rng r{seed * 0x100000001B3ull + a * 0x9E3779B97F4A7C15ull + 17};
     r.next();
-    ArenaState& s = out[a];
     memset(&s, 0, sizeof(ArenaState));
     s.tick_count = u64w(r.next() & 0xFFFFF);
     s.rng = u64w(r.next());

@@ -135,6 +135,31 @@ def unpack(words: np.ndarray, n: int) -> np.ndarray:
     return np.ascontiguousarray(words.reshape(blocks, ARENA_WORDS, 32).transpose(0, 2, 1)).reshape(blocks * 32, ARENA_WORDS)[:n]
 
 
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """SplitMix64's finaliser on uint64 arrays (wrapping)."""
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def decision_controls(seed: int, decision: int, n: int) -> np.ndarray:
+    """Deterministic controls of one decision for n arenas (the scheme of the reference's test controls,
+    tests/common/mod.rs:27-44: a SplitMix hash per (decision, arena, car); axes in {-1, 0, 1} from 4-bit fields, jump /
+    boost / handbrake from single bits).  Returns words (n, 16)."""
+    with np.errstate(over="ignore"):
+        a = np.arange(n, dtype=np.uint64)
+        out = np.zeros((n, NUM_CARS, CONTROL_WORDS), np.uint32)
+        for car in range(NUM_CARS):
+            key = (np.uint64(seed) << np.uint64(48)) ^ (np.uint64(decision) << np.uint64(24)) ^ (a << np.uint64(1)) ^ np.uint64(car)
+            h = _mix64(key)
+            for k in range(5):
+                out[:, car, k] = (((h >> np.uint64(4 * k)) % np.uint64(3)).astype(np.int64) - 1).astype(np.float32).view(np.uint32)
+            for k in range(3):
+                out[:, car, 5 + k] = ((h >> np.uint64(24 + k)) & np.uint64(1)).astype(np.uint32)
+    return out.reshape(n, NUM_CARS * CONTROL_WORDS)
+
+
 def random_controls(rng: np.random.Generator, n: int) -> np.ndarray:
     """Controls[n][2] as words: each axis uniform in {-1, 0, 1}, jump / boost / handbrake Bernoulli(0.5)."""
     c = np.zeros((n, NUM_CARS, CONTROL_WORDS), np.uint32)
