@@ -60,6 +60,13 @@ def lib() -> ctypes.CDLL:
         L.rsx_last_error.restype = ctypes.c_char_p
         L.rsx_build_static.argtypes = [u32p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
         L.rsx_make_states.argtypes = [u32p, u32p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
+        L.rsx_make_states_multi.argtypes = [u32p, ctypes.c_uint32, ctypes.c_void_p, u32p, ctypes.c_uint32, ctypes.c_uint64,
+                                            ctypes.POINTER(ctypes.c_float)]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.rsx_libm_host.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_uint64]
+        L.rsx_libm_hash_host.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
+        L.rsx_libm_hash_host.restype = ctypes.c_uint64
+        L.rsx_libm_chunk_hashes.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
         L.rsx_host_phase.argtypes = [ctypes.c_int, u32p, u32p]
         L.rsx_host_decide.argtypes = [u32p, u32p, u32p]
         L.rsx_host_decide.restype = ctypes.c_uint32
@@ -114,6 +121,18 @@ def make_states(sd: np.ndarray, n: int, seed: int, mix: Sequence[float] = MIX_HE
     st = np.zeros((n, ARENA_WORDS), np.uint32)
     m = (ctypes.c_float * 5)(*mix)
     check(lib().rsx_make_states(_p(sd), _p(st), n, seed, m), "rsx_make_states")
+    return st
+
+
+def make_states_multi(sds: np.ndarray, sd_index: np.ndarray, seed: int, mix: Sequence[float] = MIX_HEADLINE) -> np.ndarray:
+    """Start states with a car pairing per arena: sds (count, 317895), sd_index (n,) uint8."""
+    sds = np.ascontiguousarray(sds.reshape(-1, STATIC_WORDS), np.uint32)
+    idx = np.ascontiguousarray(sd_index, np.uint8)
+    n = idx.shape[0]
+    st = np.zeros((n, ARENA_WORDS), np.uint32)
+    m = (ctypes.c_float * 5)(*mix)
+    check(lib().rsx_make_states_multi(_p(sds.reshape(-1)), sds.shape[0], idx.ctypes.data_as(ctypes.c_void_p), _p(st), n, seed, m),
+          "rsx_make_states_multi")
     return st
 
 
