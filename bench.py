@@ -185,7 +185,8 @@ def run_ours(args):
     dctl = torch.from_numpy(ctl_host.view(np.int32)).to(dev.device)
     res = dev.alloc_result(n)
     ev = torch.zeros(n, dtype=torch.int32, device=dev.device)
-    stream = torch.cuda.ExternalStream(dev.stream_ptr(), device=dev.device)
+    stream = torch.cuda.Stream(device=dev.device)  # every launch and copy of the run goes on this stream
+    sptr = stream.cuda_stream
     counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     launches_per_step = 1 if args.mode == "plain" else 2  # the persistent path clears its queue counter first
@@ -193,20 +194,21 @@ def run_ours(args):
     def step(s, controls_ptr):
         if args.mode == "plain":
             rc = rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), args.block,
-                                              dev.stream_ptr())
+                                              sptr)
         else:
             rc = rsx.lib().rsx_sim8_persistent_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), None,
-                                                   counter.data_ptr(), sms * 4, args.block, 1, dev.stream_ptr())
+                                                   counter.data_ptr(), sms * 4, args.block, 1, sptr)
         rsx.check(rc, "decision")
 
     def barrier():
         if dist:
             dist.barrier()
 
+    torch.cuda.synchronize()
     # ---- device-resident timing (value) ----
     for s in range(args.warmup):
         step(s, dctl[s].data_ptr())
-    dev.sync()
+    stream.synchronize()
     barrier()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with Clocks(local) as clk:
@@ -215,7 +217,6 @@ def run_ours(args):
             step(args.warmup + k, dctl[args.warmup + k].data_ptr())
             evs[k + 1].record(stream)
         evs[-1].synchronize()
-    dev.sync()
     barrier()
     ms_steps = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     t_ms = sum(ms_steps)
@@ -294,9 +295,9 @@ def run_ours(args):
             "result_flags": flags,
             "ms_per_step_all": ms_steps,
         }))
+    torch.cuda.synchronize()
     ds.free()
     dsd.free()
-    dev.close()
     if dist:
         dist.destroy_process_group()
 

@@ -47,19 +47,9 @@ static int fail(cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return fail(e_, #x); \
   } while (0)
 
-static int configure_current(void) {
-  static std::once_flag once[64];
-  int dev = 0;
-  RSX_CK(cudaGetDevice(&dev));
-  static int status[64];
-  std::call_once(once[dev & 63], [&] {
-    // the phases run as calls with large frames (the solver's rows, the narrowphase jobs): reserve the stack they need
-    size_t want = 32 * 1024;
-    cudaError_t e = cudaDeviceSetLimit(cudaLimitStackSize, want);
-    status[dev & 63] = e == cudaSuccess ? RSX_OK : fail(e, "cudaDeviceSetLimit(stack)");
-  });
-  return status[dev & 63];
-}
+// Local memory: the kernels' call chains are known at compile time (no recursion), so the runtime sizes each thread's
+// local memory (about 20 KB: the arena state and the solver's rows) by itself; nothing to configure per device.
+static int configure_current(void) { return RSX_OK; }
 
 extern "C" {
 
@@ -83,7 +73,9 @@ int rsx_device_create(int ordinal, rsx_device** out) {
   if (c != RSX_OK) return c;
   rsx_device* d = new rsx_device;
   d->ordinal = ordinal;
-  cudaError_t e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+  // a blocking stream: ordered with work the caller puts on the legacy default stream (torch's, for one), as the
+  // reference's cudarc context with event tracking off leaves ordering to the caller's stream use
+  cudaError_t e = cudaStreamCreate(&d->stream);
   if (e != cudaSuccess) {
     delete d;
     return fail(e, "cudaStreamCreate");

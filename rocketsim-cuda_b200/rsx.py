@@ -234,11 +234,15 @@ class SimDevice:
         return unpack(self.download_words(d), d.n)
 
     def upload_controls(self, controls: np.ndarray):
+        """Controls as device words; the copy completes before this returns (the handle's launches follow it)."""
         t = self.torch.from_numpy(np.ascontiguousarray(controls.view(np.int32))).to(self.device)
+        self.torch.cuda.current_stream(self.device).synchronize()
         return t
 
     def alloc_result(self, n: int):
-        return self.torch.zeros(n, dtype=self.torch.int32, device=self.device)
+        t = self.torch.zeros(n, dtype=self.torch.int32, device=self.device)
+        self.torch.cuda.current_stream(self.device).synchronize()
+        return t
 
     def sim8(self, states: "DeviceStates", sd: "DeviceStatic", controls, result, block: int = SIM8_BLOCK, trace=None) -> None:
         if not (1 <= block <= MAX_BLOCK):
