@@ -97,6 +97,13 @@ int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_static
                             const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid, uint32_t block,
                             uint32_t granularity, void* stream);
 
+/* The same with the register budget of the kernel (min_blocks of 64 threads resident per SM: 1 -> 255 registers,
+ * 8 -> 128, 12 -> 80, 16 -> 64) and, when d_cost is non-null, each arena's decision cost in clock cycles >> 8. */
+int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                           const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
+                           uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t granularity, uint32_t min_blocks,
+                           uint32_t* d_cost, void* stream);
+
 /* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
 /* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */
 int rsx_build_static(uint32_t* words, uint64_t seed, int preset0, int preset1);

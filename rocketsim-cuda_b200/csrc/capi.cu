@@ -13,9 +13,14 @@ cudaError_t rsx_launch_sim8(uint32_t* states, const void* sd, const void* contro
                             uint32_t block, cudaStream_t s);
 cudaError_t rsx_launch_sim8_multi(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result,
                                   uint32_t* ev_or, uint32_t n, uint32_t block, cudaStream_t s);
-cudaError_t rsx_launch_sim8_persistent(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result,
-                                       uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t gran, uint32_t grid,
-                                       uint32_t block, cudaStream_t s);
+#define RSX_DECL_PERSIST(B)                                                                                               \
+  cudaError_t rsx_launch_sim8_persistent_b##B(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls,        \
+                                              uint32_t* result, uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n, \
+                                              uint32_t gran, uint32_t grid, uint32_t block, uint32_t* cost, cudaStream_t s);
+RSX_DECL_PERSIST(1)
+RSX_DECL_PERSIST(8)
+RSX_DECL_PERSIST(12)
+RSX_DECL_PERSIST(16)
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
 cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
 cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
@@ -200,15 +205,32 @@ int rsx_sim8_multi_raw(uint32_t* d_states, uint32_t n, const void* d_statics, co
 int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
                             uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
                             uint32_t block, uint32_t granularity, void* stream) {
+  return rsx_sim8_persistent_ex(d_states, n, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, grid, block,
+                                granularity, 1, nullptr, stream);
+}
+
+int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                           uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
+                           uint32_t block, uint32_t granularity, uint32_t min_blocks, uint32_t* d_cost, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_MAX_BLOCK || (block & 31) ||
       grid == 0 || granularity == 0)
     return RSX_E_ARG;
+  if (min_blocks != 1 && min_blocks != 8 && min_blocks != 12 && min_blocks != 16) return RSX_E_ARG;
   if (n == 0) return RSX_OK;
-  int c = configure_current();
-  if (c != RSX_OK) return c;
-  RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, (cudaStream_t)stream));
-  RSX_CK(rsx_launch_sim8_persistent(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
-                                    granularity, grid, block, (cudaStream_t)stream));
+  cudaStream_t s = (cudaStream_t)stream;
+  RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
+  cudaError_t e;
+  switch (min_blocks) {
+    case 8: e = rsx_launch_sim8_persistent_b8(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
+                                              granularity, grid, block, d_cost, s); break;
+    case 12: e = rsx_launch_sim8_persistent_b12(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
+                                                granularity, grid, block, d_cost, s); break;
+    case 16: e = rsx_launch_sim8_persistent_b16(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
+                                                granularity, grid, block, d_cost, s); break;
+    default: e = rsx_launch_sim8_persistent_b1(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
+                                               granularity, grid, block, d_cost, s); break;
+  }
+  RSX_CK(e);
   return RSX_OK;
 }
 

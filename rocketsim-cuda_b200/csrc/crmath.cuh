@@ -258,6 +258,109 @@ RSX_F float trig(float x, int which) {
   return from_bits(b | ((n ? 0x80000000u : 0u) ^ sx));
 }
 
+
+// ---- fast path of sin / cos: double-float (binary32 pairs, exact products by FMA) with a rounding test ----------------
+// For |x| <= 64: x = k pi/2 + r (Cody-Waite with pi/2 in three parts, the first two short enough that k * part is exact),
+// then sin and cos of r by their Taylor polynomials, the leading coefficients as float pairs.  The value carries a proven
+// error bound; when the bound does not separate it from the nearest half-way point between two floats, the exact
+// fixed-point path above decides.  Coefficients: -1/3!, 1/5!, ... and -1/2!, 1/4!, ... as (hi, lo) float pairs.
+RSX_TABLE uint32_t kSinC[7][2] = {{0xbe2aaaabu, 0x31aaaaabu}, {0x3c088889u, 0xafeeeeefu}, {0xb9500d01u, 0x2c3fcbfdu}, {0x3638ef1du, 0x292ad8e6u}, {0xb2d7322bu, 0x00000000u}, {0x2f309231u, 0x00000000u}, {0xab573f9fu, 0x00000000u}};
+RSX_TABLE uint32_t kCosC[8][2] = {{0xbf000000u, 0x00000000u}, {0x3d2aaaabu, 0xb0aaaaabu}, {0xbab60b61u, 0x2e13e93fu}, {0x37d00d01u, 0xaabfcbfdu}, {0xb493f27eu, 0x00000000u}, {0x310f76c7u, 0x00000000u}, {0xad49cba5u, 0x00000000u}, {0x29573f9fu, 0x00000000u}};
+RSX_TABLE uint32_t kPio2Split[3] = {0x3fc90f80u, 0x37354400u, 0x2e85a309u};  // |pi/2 - sum| < 1.218e-18
+
+struct DF { float h, l; };
+RSX_F DF two_prod(float a, float b) {
+  float p = fmul(a, b);
+  return {p, ffma(a, b, fneg(p))};
+}
+RSX_F DF two_sum(float a, float b) {
+  float s = fadd(a, b), bb = fsub(s, a);
+  return {s, fadd(fsub(a, fsub(s, bb)), fsub(b, bb))};
+}
+RSX_F DF quick_sum(float a, float b) {  // |a| >= |b|
+  float s = fadd(a, b);
+  return {s, fsub(b, fsub(s, a))};
+}
+RSX_F DF df_add(DF a, DF b) {
+  DF s = two_sum(a.h, b.h);
+  return quick_sum(s.h, fadd(s.l, fadd(a.l, b.l)));
+}
+RSX_F DF df_mul(DF a, DF b) {
+  DF p = two_prod(a.h, b.h);
+  return quick_sum(p.h, ffma(a.h, b.l, ffma(a.l, b.h, p.l)));
+}
+RSX_F DF df_mul_f(DF a, float b) {
+  DF p = two_prod(a.h, b);
+  return quick_sum(p.h, ffma(a.l, b, p.l));
+}
+RSX_F DF df_c(const uint32_t c[2]) { return {from_bits(c[0]), from_bits(c[1])}; }
+
+// half the gap from |h| to the neighbouring float on the side of l (a quarter ulp below a power of two)
+RSX_F float half_gap(float h, float l) {
+  uint32_t a = bits(h) & 0x7FFFFFFFu;
+  float ulp = from_bits((a & 0x7F800000u) - (23u << 23));
+  bool toward_zero = (bits(h) ^ bits(l)) >> 31;
+  return ((a & 0x7FFFFFu) == 0 && toward_zero) ? fmul(ulp, 0.25f) : fmul(ulp, 0.5f);
+}
+// the float nearest to h + l when the exact value is within err of h + l and that decides it; else false
+RSX_F bool rounds_to(DF v, float err, float* out) {
+  if (fadd(fabs_(v.l), err) < fmul(half_gap(v.h, v.l), 0.9999f)) {
+    *out = v.h;
+    return true;
+  }
+  return false;
+}
+
+// sin and cos of |x| in [2^-14, 64]: false when the fast path cannot decide one of the two it was asked for
+RSX_F float round_nearest(float v) {  // v < 2^22: the nearest integer, ties away (only the quadrant's parity matters)
+  return i2f(f2i(fadd(v, 0.5f)));
+}
+RSX_F bool sincos_fast(float ax, bool want_s, bool want_c, float* s_out, float* c_out) {
+  float rh = ax, rl = 0.0f, red_err = 0.0f;
+  int q = 0;
+  if (ax > 0.78539816f) {
+    float kf = round_nearest(fmul(ax, from_bits(0x3f22f983u)));
+    q = (int)kf & 3;
+    float t1 = ffma(fneg(kf), from_bits(kPio2Split[0]), ax);          // exact
+    DF r = two_sum(t1, fneg(fmul(kf, from_bits(kPio2Split[1]))));     // k * part2 exact
+    DF p3 = two_prod(kf, from_bits(kPio2Split[2]));
+    r = df_add(r, DF{fneg(p3.h), fneg(p3.l)});
+    rh = r.h;
+    rl = r.l;
+    red_err = fmul(kf, 2e-18f);                                        // k (pi/2 - the three parts) and the rounding below
+    red_err = fadd(red_err, fmul(fabs_(rh), 1e-14f));
+  }
+  DF y = two_prod(rh, rh);
+  float yh = y.h;
+  // sin(rh) = rh + rh * y * Q(y)
+  float ts = fadd(from_bits(kSinC[4][0]), fmul(yh, fadd(from_bits(kSinC[5][0]), fmul(yh, from_bits(kSinC[6][0])))));
+  DF qs = df_add(df_c(kSinC[3]), df_mul_f(y, ts));
+  qs = df_add(df_c(kSinC[2]), df_mul(y, qs));
+  qs = df_add(df_c(kSinC[1]), df_mul(y, qs));
+  qs = df_add(df_c(kSinC[0]), df_mul(y, qs));
+  DF cx = df_mul_f(df_mul(y, qs), rh);
+  // cos(rh) = 1 + y * P(y)
+  float tc = fadd(from_bits(kCosC[4][0]), fmul(yh, fadd(from_bits(kCosC[5][0]), fmul(yh, fadd(from_bits(kCosC[6][0]), fmul(yh, from_bits(kCosC[7][0])))))));
+  DF pc = df_add(df_c(kCosC[3]), df_mul_f(y, tc));
+  pc = df_add(df_c(kCosC[2]), df_mul(y, pc));
+  pc = df_add(df_c(kCosC[1]), df_mul(y, pc));
+  pc = df_add(df_c(kCosC[0]), df_mul(y, pc));
+  DF yp = df_mul(y, pc);
+  DF C = quick_sum(1.0f, yp.h);
+  C = quick_sum(C.h, fadd(C.l, yp.l));
+  // the low part of the reduced argument: sin(rh + rl) = sin rh + rl cos rh, cos(rh + rl) = cos rh - rl sin rh
+  DF S = two_sum(rh, cx.h);
+  S = quick_sum(S.h, fadd(S.l, fadd(cx.l, fmul(rl, C.h))));
+  C = quick_sum(C.h, fsub(C.l, fmul(rl, fadd(rh, cx.h))));
+  // quadrant
+  DF vs = (q == 0) ? S : (q == 1) ? C : (q == 2) ? DF{fneg(S.h), fneg(S.l)} : DF{fneg(C.h), fneg(C.l)};
+  DF vc = (q == 0) ? C : (q == 1) ? DF{fneg(S.h), fneg(S.l)} : (q == 2) ? DF{fneg(C.h), fneg(C.l)} : S;
+  bool ok = true;
+  if (want_s) ok = ok && rounds_to(vs, fadd(fmul(fabs_(vs.h), 1e-12f), red_err), s_out);
+  if (want_c) ok = ok && rounds_to(vc, fadd(fmul(fabs_(vc.h), 1e-12f), red_err), c_out);
+  return ok;
+}
+
 // ---- atan2 ---------------------------------------------------------------------------------------------------------
 
 // atan(t) for t = m * 2^te with m in [1, 2) (fixed point) and t <= 1, as an absolute fixed-point value; for tiny t the
@@ -495,7 +598,7 @@ RSX_F float powf_cr(float x, float y) {
 // ---- the auto-flip helpers: float(correctly rounded double) of atan2 and hypot ---------------------------------------
 
 // (float)(double atan2(a0, a1)) for float a0, a1
-RSX_F float atan2_via_double(float a0, float a1) {
+RSX_HD RSX_NOINL inline float atan2_via_double(float a0, float a1) {
   uint32_t by = bits(a0), bx = bits(a1), ay = by & 0x7FFFFFFFu, ax = bx & 0x7FFFFFFFu, sy = by & 0x80000000u;
   bool xneg = (bx >> 31) != 0;
   if (ay > 0x7F800000u || ax > 0x7F800000u || ay == 0 || ax == 0 || ay == 0x7F800000u || ax == 0x7F800000u)
@@ -506,7 +609,7 @@ RSX_F float atan2_via_double(float a0, float a1) {
 }
 
 // (float)(correctly rounded double hypot(a, b)) for float a, b, by integer square root
-RSX_F float hypot_via_double(float a, float b) {
+RSX_HD RSX_NOINL inline float hypot_via_double(float a, float b) {
   uint32_t ua = bits(a) & 0x7FFFFFFFu, ub = bits(b) & 0x7FFFFFFFu;
   if (ua >= 0x7F800000u || ub >= 0x7F800000u) {
     if (ua == 0x7F800000u || ub == 0x7F800000u) return from_bits(0x7F800000u);
@@ -559,10 +662,36 @@ RSX_F float hypot_via_double(float a, float b) {
 
 }  // namespace crm
 
-RSX_F float cr_sin(float x) { return crm::trig(x, 0); }
-RSX_F float cr_cos(float x) { return crm::trig(x, 1); }
-RSX_F float cr_tan(float x) { return crm::trig(x, 2); }
-RSX_F float cr_atan2(float y, float x) { return crm::atan2f_cr(y, x); }
-RSX_F float cr_pow(float x, float y) { return crm::powf_cr(x, y); }
+// out of line on the device: one copy of each function serves every call site (the kernels' code must stay small
+// enough for the instruction caches of warps in different phases)
+RSX_HD RSX_NOINL inline void cr_sincos(float x, float* s, float* c) {
+  uint32_t ax = bits(x) & 0x7FFFFFFFu;
+  if (ax >= 0x38800000u && ax <= 0x42800000u) {  // 2^-14 <= |x| <= 64
+    float ss, cc;
+    if (crm::sincos_fast(from_bits(ax), true, true, &ss, &cc)) {
+      *s = from_bits(bits(ss) ^ (bits(x) & 0x80000000u));
+      *c = cc;
+      return;
+    }
+  }
+  *s = crm::trig(x, 0);
+  *c = crm::trig(x, 1);
+}
+RSX_HD RSX_NOINL inline float cr_sin(float x) {
+  uint32_t ax = bits(x) & 0x7FFFFFFFu;
+  float ss, cc;
+  if (ax >= 0x38800000u && ax <= 0x42800000u && crm::sincos_fast(from_bits(ax), true, false, &ss, &cc))
+    return from_bits(bits(ss) ^ (bits(x) & 0x80000000u));
+  return crm::trig(x, 0);
+}
+RSX_HD RSX_NOINL inline float cr_cos(float x) {
+  uint32_t ax = bits(x) & 0x7FFFFFFFu;
+  float ss, cc;
+  if (ax >= 0x38800000u && ax <= 0x42800000u && crm::sincos_fast(from_bits(ax), false, true, &ss, &cc)) return cc;
+  return crm::trig(x, 1);
+}
+RSX_HD RSX_NOINL inline float cr_tan(float x) { return crm::trig(x, 2); }
+RSX_HD RSX_NOINL inline float cr_atan2(float y, float x) { return crm::atan2f_cr(y, x); }
+RSX_HD RSX_NOINL inline float cr_pow(float x, float y) { return crm::powf_cr(x, y); }
 
 }  // namespace rsx

@@ -185,20 +185,22 @@ RSX_F void force_activate(Body& b) {
 
 // ---- the quaternion integrator (transform_util.rs) ----
 RSX_F float motion_threshold() { return from_bits(0x3F490FDBu); }  // FRAC_PI_4
-RSX_F void integrate(Aff& xf, Q4& rot, V3 lin_vel, V3 ang_vel, float dt) {
+RSX_HD RSX_NOINL inline void integrate(Aff& xf, Q4& rot, V3 lin_vel, V3 ang_vel, float dt) {
   xf.t = xf.t + lin_vel * dt;
   float angle = len(ang_vel);
   if (fmul(angle, dt) > motion_threshold()) angle = fdiv(motion_threshold(), dt);
   float half = fmul(fmul(angle, dt), 0.5f);
-  float k;
+  float k, sh, ch;
   if (angle < 0.001f) {
     float t3 = fmul(fmul(dt, dt), dt);
     k = fsub(fmul(0.5f, dt), fmul(fmul(fmul(t3, 0.020833334f), angle), angle));
+    ch = cr_cos(half);
   } else {
-    k = fdiv(cr_sin(half), angle);
+    cr_sincos(half, &sh, &ch);
+    k = fdiv(sh, angle);
   }
   V3 ax = ang_vel * k;
-  Q4 dorn = {ax.x, ax.y, ax.z, cr_cos(half)};
+  Q4 dorn = {ax.x, ax.y, ax.z, ch};
   rot = qnormalize(dorn * rot);
   xf.m = m3_from_quat(rot);
 }

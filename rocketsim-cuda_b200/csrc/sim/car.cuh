@@ -22,7 +22,7 @@ RSX_F int32_t angle_units(float a0, float a1) {
   float v = fadd(fmul(u, 2.0f), 0.5f);
   return f2i(round_even(v)) >> 1;
 }
-RSX_F float autoflip_sign(const StaticData& D, const M3& r) {
+RSX_HD RSX_NOINL inline float autoflip_sign(const StaticData& D, const M3& r) {
   int32_t yaw = angle_units(r.c0.y, r.c0.x);
   float l = crm::hypot_via_double(r.c0.x, r.c0.y);
   int32_t pitch = angle_units(r.c0.z, l);
@@ -65,7 +65,10 @@ RSX_F uint64_t wy_mod(U64W* st, uint64_t n) {
 
 // Mat3A::from_euler(ZYX, yaw, 0, 0) in glam's order
 RSX_F M3 yaw_matrix(float yaw) {
-  float si = cr_sin(yaw), ci = cr_cos(yaw), sj = cr_sin(0.0f), cj = cr_cos(0.0f), sh = cr_sin(0.0f), ch = cr_cos(0.0f);
+  float si, ci, sj, cj, sh, ch;
+  cr_sincos(yaw, &si, &ci);
+  cr_sincos(0.0f, &sj, &cj);
+  cr_sincos(0.0f, &sh, &ch);
   float cc = fmul(ci, ch), cs = fmul(ci, sh), sc = fmul(si, ch), ss = fmul(si, sh);
   return M3{V3{fmul(cj, ci), fmul(cj, si), fneg(sj)}, V3{fsub(fmul(sj, cs), sc), fadd(fmul(sj, ss), cc), fmul(cj, sh)},
             V3{fadd(fmul(sj, cc), ss), fsub(fmul(sj, sc), cs), fmul(cj, ch)}};
@@ -81,7 +84,7 @@ RSX_F void sync_car_body(Car& car, Body& rb, const BodyConst& bc) {
   car.vel_impulse_cache = vzero();
 }
 
-RSX_F void respawn(ArenaState& S, const StaticData& D, int ci, float boost) {
+RSX_HD RSX_NOINL inline void respawn(ArenaState& S, const StaticData& D, int ci, float boost) {
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   Body& rb = S.bodies[slot(D, cc.body)];
@@ -212,11 +215,12 @@ RSX_F void wheel_friction_curves(Wheel& w, const View& ch, V3 cxf_t, V3 cn, floa
 }
 
 RSX_F V3 steered_axle(const Aff& cxf, float angle) {
-  float s = cr_sin(fmul(angle, 0.5f)), c = cr_cos(fmul(angle, 0.5f));
+  float s, c;
+  cr_sincos(fmul(angle, 0.5f), &s, &c);
   return qrotate(quat_axis_sc(cxf.m.c2, s, c), cxf.m.c1);
 }
 
-RSX_F void vehicle_update(ArenaState& S, const StaticData& D, int ci, float dt, float hb, float thr, bool three) {
+RSX_HD RSX_NOINL inline void vehicle_update(ArenaState& S, const StaticData& D, int ci, float dt, float hb, float thr, bool three) {
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   const uint32_t cidx = cc.body;

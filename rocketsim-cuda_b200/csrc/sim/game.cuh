@@ -225,7 +225,7 @@ RSX_F bool in_rect_cone(V3 fwd, V3 right, V3 up, V3 delta, bool reverse, float y
   return fabs_(dot(d, right)) <= fmul(f, cr_tan(fmul(yaw_deg, rpd))) && fabs_(dot(d, up)) <= fmul(f, cr_tan(fmul(pitch_deg, rpd)));
 }
 
-RSX_F void ball_hit(ArenaState& S, const StaticData& D, int ci) {
+RSX_HD RSX_NOINL inline void ball_hit(ArenaState& S, const StaticData& D, int ci) {
   Car& car = S.cars[ci];
   Body& rb = S.bodies[0];
   V3 fwd = car.rot.c0;
@@ -243,7 +243,7 @@ RSX_F void ball_hit(ArenaState& S, const StaticData& D, int ci) {
   }
 }
 
-RSX_F void car_car_hit(ArenaState& S, const StaticData& D, int c1, int c2, const RecPoint& mp) {
+RSX_HD RSX_NOINL inline void car_car_hit(ArenaState& S, const StaticData& D, int c1, int c2, const RecPoint& mp) {
   int att = c1, vic = c2;
   if (S.cars[vic].is_demoed || S.cars[att].is_demoed) return;
   for (int sw = 0; sw < 2; ++sw) {
@@ -412,7 +412,7 @@ RSX_F int pad_winner(const ArenaState& S, int p, float mx) {
     if (pad_can_take(S.cars[t.car[k]], mx)) return (int)t.car[k];
   return -1;
 }
-RSX_F void pads_tick(ArenaState& S, const StaticData& D) {
+RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
   const float mx = D.mut[M_MAX_BOOST];
   int touching[kCars] = {-1, -1};
   int winner[kPads];

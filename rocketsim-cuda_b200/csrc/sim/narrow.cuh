@@ -82,7 +82,7 @@ RSX_F uint32_t add_point_nocb(const StaticData& D, Manifold& m, const MPoint& np
   m.pts[m.n] = np;
   return m.n++;
 }
-RSX_F void refresh_points(const ArenaState& S, const StaticData& D, Manifold& m, uint32_t b0, uint32_t b1) {
+RSX_HD RSX_NOINL inline void refresh_points(const ArenaState& S, const StaticData& D, Manifold& m, uint32_t b0, uint32_t b1) {
   if (m.n == 0) return;
   Aff ta = body_xf(S, D, b0), tb = body_xf(S, D, b1);
   for (uint32_t i = 0; i < m.n; ++i) {
@@ -104,7 +104,7 @@ RSX_F void refresh_points(const ArenaState& S, const StaticData& D, Manifold& m,
     if (dot(diff, diff) > cbt2) point_swap_remove(m, (uint32_t)i);
   }
 }
-RSX_F void merge_points(const StaticData& D, Manifold& m, const Manifold& o) {
+RSX_HD RSX_NOINL inline void merge_points(const StaticData& D, Manifold& m, const Manifold& o) {
   if (m.n == 0) {
     for (uint32_t i = 0; i < o.n; ++i) m.pts[m.n++] = o.pts[i];
   } else {
@@ -161,7 +161,8 @@ RSX_F bool clamp_normal(V3 edge, V3 tn, V3 ln, float corrected, V3* out) {
   float cur = edge_angle(ec, tn, ln);
   if ((corrected < 0.0f && cur < corrected) || (corrected >= 0.0f && cur > corrected)) {
     float da = fsub(corrected, cur);
-    float s = cr_sin(fmul(da, 0.5f)), co = cr_cos(fmul(da, 0.5f));
+    float s, co;
+    cr_sincos(fmul(da, 0.5f), &s, &co);
     V3 v = normalize(edge) * vs(s);
     *out = qrotate(Q4{v.x, v.y, v.z, co}, ln);
     return true;
@@ -169,7 +170,7 @@ RSX_F bool clamp_normal(V3 edge, V3 tn, V3 ln, float corrected, V3* out) {
   return false;
 }
 RSX_F V3 tri_edge_vec(const Tri& t, int i) { return i == 0 ? t.p1 - t.p0 : (i == 1 ? t.p2 - t.p1 : t.p0 - t.p2); }
-RSX_F void edge_block(MPoint* cp, const Aff& mt, const Tri& tri, int edge_no, float angle, uint32_t flags, uint32_t cflag, uint32_t sflag,
+RSX_HD RSX_NOINL inline void edge_block(MPoint* cp, const Aff& mt, const Tri& tri, int edge_no, float angle, uint32_t flags, uint32_t cflag, uint32_t sflag,
                       V3 lcn, bool recompute, bool* concave) {
   if (angle == 0.0f) {
     *concave = true;
@@ -179,7 +180,8 @@ RSX_F void edge_block(MPoint* cp, const Aff& mt, const Tri& tri, int edge_no, fl
   float swf = fsub(fmul(convex ? 1.0f : 0.0f, 2.0f), 1.0f);
   V3 edge = -tri_edge_vec(tri, edge_no);
   V3 na = vs(swf) * tri.n;
-  float s = cr_sin(fmul(angle, 0.5f)), co = cr_cos(fmul(angle, 0.5f));
+  float s, co;
+  cr_sincos(fmul(angle, 0.5f), &s, &co);
   V3 axs = normalize(edge) * vs(s);
   V3 cnb = qrotate(Q4{axs.x, axs.y, axs.z, co}, tri.n);
   if (flags & sflag) cnb *= -1.0f;
@@ -198,7 +200,7 @@ RSX_F void edge_block(MPoint* cp, const Aff& mt, const Tri& tri, int edge_no, fl
     cp->local_b = inv_xform(mt, cp->world_b);
   }
 }
-RSX_F void adjust_internal_edge(const StaticData& D, MPoint* cp, uint32_t mesh_body, uint32_t idx) {
+RSX_HD RSX_NOINL inline void adjust_internal_edge(const StaticData& D, MPoint* cp, uint32_t mesh_body, uint32_t idx) {
   const MeshInfo& mesh = D.meshes[mesh_body];
   const TriInfo& info = D.infos[mesh.tri_first + idx];
   const Tri& tri = D.tris[mesh.tri_first + idx];
@@ -278,7 +280,7 @@ RSX_F void tracker_retained(Ctx& c, const MPoint& mp, uint32_t a, uint32_t b) {
 }
 
 // add_contact_point: a new point of the pair (body0, body1) into manifold m, with the tracker's callback
-RSX_F void add_contact(Ctx& c, Manifold& m, uint32_t b0, uint32_t b1, V3 n_b, V3 p_world, float depth, int32_t idx) {
+RSX_HD RSX_NOINL inline void add_contact(Ctx& c, Manifold& m, uint32_t b0, uint32_t b1, V3 n_b, V3 p_world, float depth, int32_t idx) {
   if (depth > breaking(c.D, m)) return;
   V3 pa = p_world + n_b * depth;
   MPoint np = {};
@@ -298,7 +300,7 @@ RSX_F void add_contact(Ctx& c, Manifold& m, uint32_t b0, uint32_t b1, V3 n_b, V3
 }
 
 // ---- convex (ball sphere or car box child) against a plane ----
-RSX_F bool alg_convex_plane(Ctx& c, uint32_t obj, uint32_t plane_obj, const Aff& wt, bool box, Manifold* out) {
+RSX_HD RSX_NOINL inline bool alg_convex_plane(Ctx& c, uint32_t obj, uint32_t plane_obj, const Aff& wt, bool box, Manifold* out) {
   const Plane& pl = c.D.planes[plane_obj - kMeshes];
   const BodyConst& bc = c.D.bodies[obj];
   Box3 cb = box ? box_from_half(bc.box_half, bc.box_margin, wt) : sphere_box(bc.sphere_margin, wt.t);
@@ -328,7 +330,7 @@ RSX_F bool alg_convex_plane(Ctx& c, uint32_t obj, uint32_t plane_obj, const Aff&
 }
 
 // ---- ball against a car box ----
-RSX_F bool alg_sphere_box(Ctx& c, uint32_t sph, uint32_t car, Manifold* out) {
+RSX_HD RSX_NOINL inline bool alg_sphere_box(Ctx& c, uint32_t sph, uint32_t car, Manifold* out) {
   Aff st = body_xf(c.S, c.D, sph);
   float radius = c.D.bodies[sph].sphere_margin;
   if (!box_overlap(sphere_box(radius, st.t), body_box(c.S, c.D, car))) return false;
@@ -660,7 +662,7 @@ RSX_NOINL RSX_HD inline void box_box_points(Ctx& c, Obb o1, M3 r1t, Obb o2, M3 r
     add_contact(c, *m, b1, b2, -hit.n, hit.code < 4 ? pw : pw - hit.n * dep[id], fneg(dep[id]), -1);
   }
 }
-RSX_F bool alg_box_box(Ctx& c, uint32_t ba, uint32_t bb, Manifold* out) {
+RSX_HD RSX_NOINL inline bool alg_box_box(Ctx& c, uint32_t ba, uint32_t bb, Manifold* out) {
   if (!box_overlap(body_box(c.S, c.D, ba), body_box(c.S, c.D, bb))) return false;
   Aff ta = child_xf(c.S, c.D, ba), tb = child_xf(c.S, c.D, bb);
   M3 ainv = transpose(ta.m);
@@ -724,7 +726,7 @@ RSX_F float seg_dist2(V3 from, V3 to, V3 p, V3* nearest) {
   *nearest = from + vs(t) * v;
   return dot(diff, diff);
 }
-RSX_F bool sphere_triangle(const Tri& t, V3 center, float radius, float rt, float rt2, SphereTriHit* out) {
+RSX_HD RSX_NOINL inline bool sphere_triangle(const Tri& t, V3 center, float radius, float rt, float rt2, SphereTriHit* out) {
   V3 to_c = center - t.p0;
   float dp = dot(to_c, t.n);
   if (dp < 0.0f) return false;
@@ -874,7 +876,7 @@ RSX_F void push_active(ArenaState& S, uint32_t i) {
   S.active[S.n_active++] = i;
 }
 // the second half: merge the fresh manifold into the retained one (or insert it), then mark it active
-RSX_F void near_tail(Ctx& c, uint32_t rb0, uint32_t rb1, int32_t cached, bool has_fresh, const Manifold& fresh) {
+RSX_HD RSX_NOINL inline void near_tail(Ctx& c, uint32_t rb0, uint32_t rb1, int32_t cached, bool has_fresh, const Manifold& fresh) {
   ArenaState& S = c.S;
   int32_t act;
   if (cached >= 0) {

@@ -125,7 +125,7 @@ RSX_F uint32_t node_mask(const WideNode& n, const Box3& b) {
   }
   return m & n.valid;
 }
-RSX_F void ray_mesh(const StaticData& D, const MeshInfo& mesh, LocalRays* lr, RayBox* rb) {
+RSX_HD RSX_NOINL inline void ray_mesh(const StaticData& D, const MeshInfo& mesh, LocalRays* lr, RayBox* rb) {
   if (!box_overlap(rb->box, mesh.root_box)) return;
   float o[3][4], inv[3][4];
   raybox_dirs(*rb, o, inv);
@@ -246,7 +246,7 @@ RSX_F void ray_plane(const Plane& pl, LocalRays* lr, const RayBox& rb) {
 }
 
 // ---- a car's box (a compound of one rounded box) ----
-RSX_F bool rounded_box_solve(V3 src, V3 dir, float dist, V3 inner, float margin, float* t_out, V3* n_out) {
+RSX_HD RSX_NOINL inline bool rounded_box_solve(V3 src, V3 dir, float dist, V3 inner, float margin, float* t_out, V3* n_out) {
   float pts[8];
   for (int i = 0; i < 8; ++i) pts[i] = 0.0f;
   pts[1] = dist;
@@ -321,7 +321,7 @@ RSX_F bool rounded_box_solve(V3 src, V3 dir, float dist, V3 inner, float margin,
   }
   return false;
 }
-RSX_F void ray_box_one(const BodyConst& bc, LocalRays* lr, V3 src, V3 tgt, int ri) {
+RSX_HD RSX_NOINL inline void ray_box_one(const BodyConst& bc, LocalRays* lr, V3 src, V3 tgt, int ri) {
   const Box3& la = bc.compound_box;
   V3 delta = tgt - src;
   float dist = len(delta);
@@ -383,7 +383,7 @@ RSX_F void ray_box(const BodyConst& bc, LocalRays* lr, const RayBox& rb) {
 }
 
 // ---- one candidate body (collision_world quad_ray_test) ----
-RSX_F void ray_body(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk) {
+RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk) {
   View co = view(S, D, w);
   const BodyConst& bc = D.bodies[w];
   V3 fl[4], tl[4];

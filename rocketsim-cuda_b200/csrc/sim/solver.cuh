@@ -380,21 +380,6 @@ RSX_F void emit_special(Solver& sv, ArenaState& S, const StaticData& D, const Sp
   sv.fric[sv.nf++] = friction_row(ia, ib, sa, sb, s0, s1, r1, r2, cp.friction, lat, fi);
 }
 
-RSX_F void solver_integrate(Aff& xf, Q4& rot, V3 lin, V3 ang, float dt) {
-  xf.t += lin * dt;
-  float angle = len(ang);
-  const float thr = 0.78539816339744830962f;
-  if (fmul(angle, dt) > thr) angle = fdiv(thr, dt);
-  float half = fmul(fmul(angle, dt), 0.5f);
-  float sc;
-  if (angle < 0.001f) sc = fsub(fmul(0.5f, dt), fmul(fmul(fmul(fmul(fmul(dt, dt), dt), 0.020833334f), angle), angle));
-  else sc = fdiv(cr_sin(half), angle);
-  V3 ax = ang * sc;
-  Q4 dorn = {ax.x, ax.y, ax.z, cr_cos(half)};
-  rot = qnormalize(dorn * rot);
-  xf.m = m3_from_quat(rot);
-}
-
 RSX_F void phase5(ArenaState& S, const StaticData& D) {
   const float dt = fdiv(1.0f, 120.0f);
   Solver sv;
@@ -495,7 +480,7 @@ RSX_F void phase5(ArenaState& S, const StaticData& D) {
         wt.t += b.push * dt;
       } else {
         Q4 q = body.quat;
-        solver_integrate(wt, q, b.push, b.turn * kSplitTurnErp, dt);
+        integrate(wt, q, b.push, b.turn * kSplitTurnErp, dt);  // transform_util.rs integrate_trans, the same steps
       }
       if ((body.flags & CF_NO_ANGULAR) == 0) body.quat = quat_from_m3(wt.m);
       body.xf = wt;
