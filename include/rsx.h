@@ -103,6 +103,11 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
                            const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
                            uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t granularity, uint32_t min_blocks,
                            uint32_t* d_cost, void* stream);
+/* Phase profile of one decision (no counterpart in the reference): d_phase_cycles[10] receives, per phase P0, P1, P2,
+ * P3a, P3b, P4, P5, P6, P7, P8, the clock cycles all warps spent in it over the 8 ticks (zeroed by the call).  The states
+ * advance by one decision; the goal state is not kept, so use it on a copy. */
+int rsx_profile_phases_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                           const rsx_controls* d_controls, uint64_t* d_phase_cycles, void* stream);
 
 /* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
 /* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */

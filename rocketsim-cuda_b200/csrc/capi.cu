@@ -24,6 +24,8 @@ RSX_DECL_PERSIST(16)
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
 cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
 cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
+cudaError_t rsx_launch_sim8_profile(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t n,
+                                    unsigned long long* prof, cudaStream_t s);
 
 
 struct rsx_device {
@@ -45,6 +47,10 @@ static thread_local char g_err[256] = "";
 static int fail(cudaError_t e, const char* where) {
   snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
   return RSX_E_CUDA;
+}
+int rsx_set_last_error(int code, const char* msg) {
+  snprintf(g_err, sizeof(g_err), "%s", msg);
+  return code;
 }
 #define RSX_CK(x)                          \
   do {                                     \
@@ -231,6 +237,16 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
                                                granularity, grid, block, d_cost, s); break;
   }
   RSX_CK(e);
+  return RSX_OK;
+}
+
+int rsx_profile_phases_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                           uint64_t* d_phase_cycles, void* stream) {
+  if (!d_states || !d_statics || !d_controls || !d_phase_cycles) return RSX_E_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  RSX_CK(cudaMemsetAsync(d_phase_cycles, 0, 10 * sizeof(uint64_t), s));
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_sim8_profile(d_states, d_statics, d_sd_index, d_controls, n, (unsigned long long*)d_phase_cycles, s));
   return RSX_OK;
 }
 
