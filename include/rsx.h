@@ -103,6 +103,16 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
                            const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
                            uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t granularity, uint32_t min_blocks,
                            uint32_t* d_cost, void* stream);
+/* The persistent decision without caller scratch (no counterpart in the reference): for callers that cannot allocate
+ * device memory (their framework owns it, or cudaMalloc / cudaFree would synchronise a real-time loop), the work-queue
+ * counter lives in a fixed 256-byte device array of the library instead of d_queue_counter.  At most 2^24 arenas,
+ * granularity 256 and grid 65,535 per call (RSX_E_ARG beyond).  The first call on a device looks the array up (make it
+ * before any stream capture); calls share the array, so calls whose launches overlap on the GPU race.  Results equal
+ * rsx_sim8_persistent_raw's. */
+int rsx_sim8_persistent_noalloc(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                                const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
+                                uint32_t grid, uint32_t block, uint32_t granularity, void* stream);
+
 /* Phase profile of one decision (no counterpart in the reference): d_phase_cycles[10] receives, per phase P0, P1, P2,
  * P3a, P3b, P4, P5, P6, P7, P8, the clock cycles all warps spent in it over the 8 ticks (zeroed by the call).  The states
  * advance by one decision; the goal state is not kept, so use it on a copy. */
