@@ -44,9 +44,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--arenas", type=int, default=ARENAS)
-    ap.add_argument("--mode", default="plain", choices=["plain", "persistent"])
-    ap.add_argument("--block", type=int, default=32)
-    ap.add_argument("--cpu-sample", type=int, default=8192, help="arenas of the CPU baseline sample")
+    ap.add_argument("--mode", default="lockstep", choices=["plain", "persistent", "lockstep"])
+    ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
+    ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
+    ap.add_argument("--split", type=int, default=1, help="lockstep: barrier after each car's pre-tick too")
+    ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain launch's comparison timing")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="reference arm: arenas per step (0: all)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline: seconds of decisions of the workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
     return ap.parse_args()
@@ -72,11 +77,11 @@ def oracle_batch():
     return L
 
 
-def cpu_run(L, rsx, sds, idx, st, decisions, seed):
-    """The reference's CPU build over `st` (in place) for `decisions` decisions on all host threads; returns
-    (arena-ticks/s, threads, seconds)."""
+def cpu_run(L, rsx, sds, idx, st, decisions, seed, first=0):
+    """The reference's CPU build over `st` (in place) for `decisions` decisions (controls of decisions first,
+    first + 1, ... of `seed`) on all host threads; returns (arena-ticks/s, threads, seconds)."""
     n = st.shape[0]
-    ctl = np.ascontiguousarray(np.stack([rsx.decision_controls(seed, d, n) for d in range(decisions)]))
+    ctl = np.ascontiguousarray(np.stack([rsx.decision_controls(seed, first + d, n) for d in range(decisions)]))
     sdsc = np.ascontiguousarray(sds)
     t = time.perf_counter()
     th = L.rsref_run_batch(st.ctypes.data, n, sdsc.ctypes.data, idx.ctypes.data, ctl.ctypes.data, decisions, 0, None)
@@ -94,7 +99,7 @@ class Clocks:
         q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -133,27 +138,26 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librsbatch.so not built (the reference sources were absent)"}))
         return
     n = args.arenas
-    sample = min(args.cpu_sample, n)
+    sample = n if args.cpu_sample <= 0 else min(args.cpu_sample, n)
     sds, idx, st = world(rsx, n, 0, args.seed)
-    # each step: one decision of a bounded sample of the workload's arenas (rotating through them)
+    st = np.ascontiguousarray(st[:sample])
+    idx = np.ascontiguousarray(idx[:sample])
+    # step s: one decision of the (sampled) workload with the controls the GPU arm uses for its step s
     for w in range(args.warmup):
-        lo = (w * sample) % n
-        cpu_run(L, rsx, sds, idx[lo:lo + sample], np.ascontiguousarray(st[lo:lo + sample]), 1, args.seed + w)
+        cpu_run(L, rsx, sds, idx, st, 1, args.seed * 1000, first=w)
     tot_ticks, tot_s, threads = 0, 0.0, 0
     for k in range(args.steps):
-        lo = ((args.warmup + k) * sample) % n
-        part = np.ascontiguousarray(st[lo:lo + sample])
-        v, threads, dt = cpu_run(L, rsx, sds, np.ascontiguousarray(idx[lo:lo + sample]), part, 1, args.seed + 100 + k)
+        _, threads, dt = cpu_run(L, rsx, sds, idx, st, 1, args.seed * 1000, first=args.warmup + k)
         tot_ticks += sample * 8
         tot_s += dt
     value = tot_ticks / tot_s
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": f"headline mix, {n} arenas, 7x7 car pairings; each step one decision of a {sample}-arena sample",
+        "data": "synthetic", "config": {"workload": f"headline mix, {n} arenas, 7x7 car pairings; each step one decision of {sample} of them",
                                          "arenas": n, "sample_arenas": sample},
         "cpu_baseline": {"value": value, "unit": "arena-ticks/s", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} arenas x 1 decision per step, {args.steps} steps"},
+                         "sample": f"{sample} arenas x 1 decision per step, {args.steps} steps ({tot_s:.1f} s)"},
         "e2e": {"value": value, "unit": "arena-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -189,41 +193,59 @@ def run_ours(args):
     sptr = stream.cuda_stream
     counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
     sms = torch.cuda.get_device_properties(local).multi_processor_count
-    launches_per_step = 1 if args.mode == "plain" else 2  # the persistent path clears its queue counter first
+    grid = args.grid or sms
+    words = rsx.pack(st)
 
-    def step(s, controls_ptr):
-        if args.mode == "plain":
-            rc = rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), args.block,
-                                              sptr)
-        else:
+    def step(mode, s, controls_ptr):
+        if mode == "plain":
+            rc = rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(),
+                                              args.plain_block, sptr)
+        elif mode == "persistent":
             rc = rsx.lib().rsx_sim8_persistent_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), None,
-                                                   counter.data_ptr(), sms * 4, args.block, 1, sptr)
+                                                   counter.data_ptr(), sms * 4, 32, 1, sptr)
+        else:
+            rc = rsx.lib().rsx_sim8_lockstep_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), None,
+                                                 counter.data_ptr(), grid, args.block, args.split, sptr)
         rsx.check(rc, "decision")
 
     def barrier():
         if dist:
             dist.barrier()
 
-    torch.cuda.synchronize()
-    # ---- device-resident timing (value) ----
-    for s in range(args.warmup):
-        step(s, dctl[s].data_ptr())
-    stream.synchronize()
-    barrier()
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    with Clocks(local) as clk:
+    def timed(mode, clk=None):
+        """W warm-up + K timed decisions of `mode` from the start states; per-step device ms (max over ranks summed)."""
+        rsx.check(rsx.lib().rsx_states_upload(dev.h, ds.h, rsx._p(words)), "states upload")
+        torch.cuda.synchronize()
+        for s in range(args.warmup):
+            step(mode, s, dctl[s].data_ptr())
+        stream.synchronize()
+        barrier()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        if clk:
+            clk.__enter__()
         evs[0].record(stream)
         for k in range(args.steps):
-            step(args.warmup + k, dctl[args.warmup + k].data_ptr())
+            step(mode, args.warmup + k, dctl[args.warmup + k].data_ptr())
             evs[k + 1].record(stream)
         evs[-1].synchronize()
-    barrier()
-    ms_steps = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
-    t_ms = sum(ms_steps)
-    if dist:
-        tt = torch.tensor([t_ms], device=dev.device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+        if clk:
+            clk.__exit__()
+        barrier()
+        ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+        t = sum(ms)
+        if dist:
+            tt = torch.tensor([t], device=dev.device)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, ms
+
+    # ---- the plain one-thread-per-arena launch, then this mode, each from the same start states and controls ----
+    plain = None
+    if args.mode != "plain" and not args.no_plain:
+        t_plain, _ = timed("plain")
+        plain = world_size * n * 8 * args.steps / (t_plain / 1e3)
+    clk = Clocks(local)
+    t_ms, ms_steps = timed(args.mode, clk)
     value = world_size * n * 8 * args.steps / (t_ms / 1e3)
 
     # ---- end to end through the public entry point: pinned host controls in, result words out, every step ----
@@ -234,14 +256,14 @@ def run_ours(args):
     with torch.cuda.stream(stream):
         for s in range(2):
             dctl1.copy_(pin_ctl[s], non_blocking=True)
-            step(s, dctl1.data_ptr())
+            step(args.mode, s, dctl1.data_ptr())
             pin_res.copy_(res, non_blocking=True)
         stream.synchronize()
         barrier()
         e0.record(stream)
         for k in range(args.steps):
             dctl1.copy_(pin_ctl[args.warmup + k], non_blocking=True)
-            step(args.warmup + k, dctl1.data_ptr())
+            step(args.mode, args.warmup + k, dctl1.data_ptr())
             pin_res.copy_(res, non_blocking=True)
             stream.synchronize()  # the caller reads the step's result words
         e1.record(stream)
@@ -274,24 +296,33 @@ def run_ours(args):
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         L = oracle_batch()
         if L is not None:
-            sample = min(args.cpu_sample, n)
-            part = np.ascontiguousarray(st[:sample])
-            v, th, dt = cpu_run(L, rsx, sds, np.ascontiguousarray(idx[:sample]), part, 2, 77)
-            cpu = {"value": v, "unit": "arena-ticks/s", "cores": th, "kind": "reference",
-                   "sample": f"{sample} arenas x 2 decisions of the headline workload ({dt:.1f} s)"}
+            # decisions of the whole workload from its start states until about cpu_seconds of CPU time have passed
+            part = np.ascontiguousarray(st)
+            ticks, secs, d, th = 0, 0.0, 0, 0
+            while secs < args.cpu_seconds or d < 2:
+                _, th, dt = cpu_run(L, rsx, sds, idx, part, 1, args.seed * 1000, first=d)
+                ticks += n * 8
+                secs += dt
+                d += 1
+            cpu = {"value": ticks / secs, "unit": "arena-ticks/s", "cores": th, "kind": "reference",
+                   "sample": f"{n} arenas x {d} decisions of the same workload from its start states ({secs:.1f} s)"}
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded states and arena mesh)",
             "config": {"workload": "headline: 65,536 arenas per GPU, mixed states, 7x7 car pairings, one 8-tick decision per step",
-                       "arenas_per_gpu": n, "mode": args.mode, "block": args.block,
+                       "arenas_per_gpu": n, "mode": args.mode, "block": args.block if args.mode == "lockstep" else args.plain_block,
+                       "grid": grid if args.mode == "lockstep" else None, "split": args.split if args.mode == "lockstep" else None,
                        "l2": "inputs larger than L2 (AoSoA state buffer 730 MB per GPU)", "parallelism": f"replicas x{world_size}"},
             "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * 4},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "gpu_launches": launches_per_step * args.steps,
+            "plain": None if plain is None else {"value": plain, "unit": "arena-ticks/s", "block": args.plain_block,
+                                                 "what": "one thread per arena, one launch per decision (the reference's sim8 shape)"},
+            "speedup_vs_plain": None if plain is None else value / plain,
+            "gpu_launches": args.steps,
             "result_flags": flags,
             "ms_per_step_all": ms_steps,
         }))

@@ -103,6 +103,17 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
                            const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
                            uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t granularity, uint32_t min_blocks,
                            uint32_t* d_cost, void* stream);
+/* The SM-lockstep persistent decision (no counterpart in the reference): `grid` resident blocks of `block` threads (a
+ * multiple of 32, at most RSX_LOCKSTEP_MAX_BLOCK; normally one block per SM) step their warps' arenas phase by phase
+ * together, so that all warps of an SM execute one phase's code at a time; each warp claims 32 entries of d_order
+ * (identity when null) from d_queue_counter (cleared by the call) when its arenas finish.  split 1 adds a barrier after
+ * each car's pre-tick inside P1.  Register budget by block: up to 384 threads 168 registers, 448 144, 512 128.  Results
+ * equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
+#define RSX_LOCKSTEP_MAX_BLOCK 512u
+int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                          const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
+                          uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t split, void* stream);
+
 /* The persistent decision without caller scratch (no counterpart in the reference): for callers that cannot allocate
  * device memory (their framework owns it, or cudaMalloc / cudaFree would synchronise a real-time loop), the work-queue
  * counter lives in a fixed 256-byte device array of the library instead of d_queue_counter.  At most 2^24 arenas,

@@ -21,6 +21,13 @@ RSX_DECL_PERSIST(1)
 RSX_DECL_PERSIST(8)
 RSX_DECL_PERSIST(12)
 RSX_DECL_PERSIST(16)
+#define RSX_DECL_LOCKSTEP(T)                                                                                                \
+  cudaError_t rsx_launch_sim8_lockstep_t##T(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls,         \
+                                            uint32_t* result, uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n,  \
+                                            uint32_t grid, uint32_t block, int split, cudaStream_t s);
+RSX_DECL_LOCKSTEP(384)
+RSX_DECL_LOCKSTEP(448)
+RSX_DECL_LOCKSTEP(512)
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
 cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
 cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
@@ -236,6 +243,29 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
     default: e = rsx_launch_sim8_persistent_b1(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n,
                                                granularity, grid, block, d_cost, s); break;
   }
+  RSX_CK(e);
+  return RSX_OK;
+}
+
+int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                          uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
+                          uint32_t block, uint32_t split, void* stream) {
+  if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
+      (block & 31) || grid == 0 || split > 1)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 1");
+  if (n == 0) return RSX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
+  cudaError_t e;
+  if (block <= 384)
+    e = rsx_launch_sim8_lockstep_t384(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
+                                      block, (int)split, s);
+  else if (block <= 448)
+    e = rsx_launch_sim8_lockstep_t448(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
+                                      block, (int)split, s);
+  else
+    e = rsx_launch_sim8_lockstep_t512(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
+                                      block, (int)split, s);
   RSX_CK(e);
   return RSX_OK;
 }

@@ -11,7 +11,11 @@
 
 #if defined(__CUDACC__)
 #define RSX_HD __host__ __device__
+#if defined(RSX_SOFT_INLINE)
+#define RSX_INL inline
+#else
 #define RSX_INL __forceinline__
+#endif
 #define RSX_NOINL __noinline__
 #else
 #define RSX_HD

@@ -1,0 +1,134 @@
+// The SM-lockstep persistent decision kernel.
+//
+// Why: one decision runs ~10^5 dependent instructions per arena through a simulator whose machine code is about a
+// megabyte (P1 and P3b alone are ~450 KB each), far beyond an SM's instruction cache.  When the warps of an SM drift
+// into different phases, every warp's instruction fetches evict the others' and the SM stalls on instruction misses
+// (measured on the one-thread-per-arena launch: ~26 cycles of "no instruction" stall per issued instruction, issue
+// active 4% of cycles).  Here the warps of a block step their arenas phase by phase together: a __syncthreads()
+// after each of the ten phases (and, with `split`, after each car's pre-tick inside P1), so that at any time the
+// block's warps fetch from one phase's code.
+//
+// Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
+// 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
+// launch) whenever its previous 32 arenas have finished their 8 ticks, and loads them at the next tick boundary.  The
+// block leaves when no warp holds work.  Lanes past n step a copy of their warp's first arena and store nothing.
+//
+// Results: each arena's decision is the decide() sequence of sim/physics.cuh (controls before every tick, all 8 ticks
+// stepped, the state after the first scored tick kept, event OR up to that tick), so states, result words and event
+// words equal those of every other decision kernel, whatever grid, block, split or order.
+//
+// Compiled once per register budget (RSX_LS_MAXT threads per block, one block per SM: 384 -> 168 registers,
+// 448 -> 144, 512 -> 128).
+#include "kern_common.cuh"
+
+#ifndef RSX_LS_MAXT
+#define RSX_LS_MAXT 512
+#endif
+#define RSX_CAT2(a, b) a##b
+#define RSX_CAT(a, b) RSX_CAT2(a, b)
+#define K_NAME RSX_CAT(k_sim8_lockstep_t, RSX_LS_MAXT)
+#define L_NAME RSX_CAT(rsx_launch_sim8_lockstep_t, RSX_LS_MAXT)
+
+template <int SPLIT>
+__global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const StaticData* sds, const uint8_t* sd_index,
+                                                        const Controls* controls, uint32_t* result, uint32_t* ev_or,
+                                                        const uint32_t* order, uint32_t* counter, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u;
+  ArenaState s;
+  Controls c0, c1;
+  const StaticData* D = sds;
+  uint32_t a = 0, t = 0, scored = 0, unimpl = 0, ev = 0;
+  bool live = false, have = false, ovf = false;
+  for (;;) {
+    // a warp without arenas claims the next 32 entries of the queue
+    if (!have) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(counter, 32u);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0);
+      if (base < n) {
+        uint32_t i = base + lane;
+        live = i < n;
+        uint32_t j = live ? i : base;
+        a = order ? order[j] : j;
+        D = sds + (sd_index ? sd_index[a] : 0);
+        load_tick(&s, states, a);
+        c0 = controls[(size_t)a * kCars];
+        c1 = controls[(size_t)a * kCars + 1];
+        t = 1;
+        scored = unimpl = ev = 0;
+        ovf = false;
+        have = true;
+      }
+    }
+    if (!__syncthreads_or(have)) break;
+    // one tick, phase by phase in lockstep (every thread reaches every barrier)
+    int un = 0;
+    if (have) {
+      s.cars[0].controls = c0;
+      s.cars[1].controls = c1;
+    }
+    if (SPLIT) {
+      if (have) sim::t_p0(s, *D);
+      __syncthreads();
+      if (have) {
+        sim::flip_zdamp(s, *D, 0);
+        sim::flip_zdamp(s, *D, 1);
+      }
+#pragma unroll 1
+      for (int ci = 0; ci < kCars; ++ci) {
+        if (have) {
+          uint32_t was = s.cars[ci].on_ground;
+          sim::car_pre_tick(s, *D, ci);
+          if (!was && s.cars[ci].on_ground) s.events |= 1u << (EV_LANDED + ci);
+        }
+        __syncthreads();
+      }
+#pragma unroll 1
+      for (int k = 2; k < sim::kPhases; ++k) {
+        if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
+        __syncthreads();
+      }
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < sim::kPhases; ++k) {
+        if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
+        __syncthreads();
+      }
+    }
+    // the tick hooks of decide(): event OR, goal state, and the end of the decision
+    if (have) {
+      if (scored == 0) {
+        if (un) unimpl = kUnimplemented;
+        ev |= s.events;
+        if (sim::ball_scored(s, *D)) {
+          scored = t;
+          if (live) store_tick(states, a, &s);
+          ovf = sim::any_overflow(s);
+        }
+      }
+      if (t == kTicksPerDecision) {
+        if (scored == 0) {
+          if (live) store_tick(states, a, &s);
+          ovf = sim::any_overflow(s);
+        }
+        if (live) {
+          if (ev_or) ev_or[a] = ev;
+          result[a] = scored | unimpl | (ovf ? kOverflow : 0u);
+        }
+        have = false;
+      }
+      ++t;
+    }
+  }
+}
+
+cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result, uint32_t* ev_or,
+                   const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
+  const StaticData* D = (const StaticData*)sds;
+  const Controls* C = (const Controls*)controls;
+  if (split)
+    K_NAME<1><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else
+    K_NAME<0><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  return cudaGetLastError();
+}

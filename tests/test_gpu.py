@@ -90,8 +90,10 @@ def test_sim8_matches_oracle(rsx, dev, idx):
 
 
 def test_result_independent_of_block_order_and_queue(rsx, dev):
-    """Block 32 vs 64, the multi-static kernel, and the persistent kernel over a permuted order with several queue
-    granularities give the same words (the reference's determinism test, tests/step.rs:455-506)."""
+    """Block 32 vs 64, the multi-static kernel, the persistent kernel over a permuted order with several queue
+    granularities, and the SM-lockstep kernel over several grids, blocks, barrier splits and orders (grid 2 x 64
+    threads: 4 warps take 32 claims in turn) give the same words (the reference's determinism test,
+    tests/step.rs:455-506)."""
     import torch
 
     sds = np.stack([rsx.build_static(7, p, q) for p, q in [(0, 0), (1, 2), (5, 6)]])
@@ -107,7 +109,8 @@ def test_result_independent_of_block_order_and_queue(rsx, dev):
     dperm = torch.from_numpy(perm.view(np.int32)).to(dev.device)
     counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
     variants = [("multi", 32, None, 0, 0), ("multi", 64, None, 0, 0), ("persist", 32, dperm, 148, 1), ("persist", 64, dperm, 37, 3),
-                ("persist", 32, None, 7, 2)]
+                ("persist", 32, None, 7, 2), ("lock", 512, dperm, 148, 1), ("lock", 384, None, 3, 0), ("lock", 448, dperm, 2, 1),
+                ("lock", 64, dperm, 2, 1), ("lock", 480, None, 1, 0)]
     for kind, block, order, grid, gran in variants:
         ds = dev.upload_states(st)
         res = dev.alloc_result(n)
@@ -117,6 +120,10 @@ def test_result_independent_of_block_order_and_queue(rsx, dev):
             if kind == "multi":
                 rc = rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), ev.data_ptr(),
                                                   block, dev.stream_ptr())
+            elif kind == "lock":
+                rc = rsx.lib().rsx_sim8_lockstep_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), ev.data_ptr(),
+                                                     order.data_ptr() if order is not None else None, counter.data_ptr(), grid, block, gran,
+                                                     dev.stream_ptr())
             else:
                 rc = rsx.lib().rsx_sim8_persistent_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), ev.data_ptr(),
                                                        order.data_ptr() if order is not None else None, counter.data_ptr(), grid, block,
