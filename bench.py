@@ -44,7 +44,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--arenas", type=int, default=ARENAS)
-    ap.add_argument("--mode", default="lockstep", choices=["plain", "persistent", "lockstep"])
+    ap.add_argument("--mode", default="binned", choices=["plain", "lockstep", "binned"],
+                    help="binned: autotuned lockstep kernel with the learned binning among its candidates")
+    ap.add_argument("--threshold", type=float, default=0.5, help="binned without the autotuner: predicted-contact threshold")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch the timed decisions one by one instead of as CUDA graphs")
+    ap.add_argument("--train-decisions", type=int, default=32, help="decisions of exact labels for the predictor")
+    ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
     ap.add_argument("--split", type=int, default=1, help="lockstep: barrier after each car's pre-tick too")
@@ -165,6 +171,8 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import rsx
+    import predictor as P
+    from runner import DecisionRunner
 
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -181,98 +189,149 @@ def run_ours(args):
     dev = rsx.SimDevice(local)
     n = args.arenas
     sds, idx, st = world(rsx, n, rank, args.seed)
-    dsd = dev.upload_static(sds)
-    ds = dev.upload_states(st)
-    didx = torch.from_numpy(idx).to(dev.device)
+    run = DecisionRunner(dev, sds, idx, st)
+    stream = run.stream
     steps = args.warmup + args.steps
     ctl_host = np.stack([rsx.decision_controls(args.seed * 1000 + rank, s, n) for s in range(steps)])  # (steps, n, 16)
     dctl = torch.from_numpy(ctl_host.view(np.int32)).to(dev.device)
-    res = dev.alloc_result(n)
-    ev = torch.zeros(n, dtype=torch.int32, device=dev.device)
-    stream = torch.cuda.Stream(device=dev.device)  # every launch and copy of the run goes on this stream
-    sptr = stream.cuda_stream
-    counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
-    sms = torch.cuda.get_device_properties(local).multi_processor_count
-    grid = args.grid or sms
-    words = rsx.pack(st)
-
-    def step(mode, s, controls_ptr):
-        if mode == "plain":
-            rc = rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(),
-                                              args.plain_block, sptr)
-        elif mode == "persistent":
-            rc = rsx.lib().rsx_sim8_persistent_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), None,
-                                                   counter.data_ptr(), sms * 4, 32, 1, sptr)
-        else:
-            rc = rsx.lib().rsx_sim8_lockstep_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), controls_ptr, res.data_ptr(), ev.data_ptr(), None,
-                                                 counter.data_ptr(), grid, args.block, args.split, sptr)
-        rsx.check(rc, "decision")
+    torch.cuda.synchronize()
+    start = run.snapshot()
 
     def barrier():
         if dist:
             dist.barrier()
 
-    def timed(mode, clk=None):
-        """W warm-up + K timed decisions of `mode` from the start states; per-step device ms (max over ranks summed)."""
-        rsx.check(rsx.lib().rsx_states_upload(dev.h, ds.h, rsx._p(words)), "states upload")
-        torch.cuda.synchronize()
+    def reduce_max(x):
+        if not dist:
+            return x
+        tt = torch.tensor([x], device=dev.device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    def timed(config, graph=False, clk=None):
+        """W warm-up + K timed decisions of `config` from the start states; (device ms of the K, per-step ms)."""
+        run.restore(start)
         for s in range(args.warmup):
-            step(mode, s, dctl[s].data_ptr())
+            run.step(dctl[s].data_ptr(), config)
+        graphs = []
+        if graph:  # the K timed decisions as CUDA graphs of up to 16 decisions (captured, not run, here)
+            for g0 in range(0, args.steps, 16):
+                ptrs = [dctl[args.warmup + k].data_ptr() for k in range(g0, min(args.steps, g0 + 16))]
+                graphs.append((len(ptrs), run.capture(ptrs, config)))
         stream.synchronize()
         barrier()
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         if clk:
             clk.__enter__()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         evs[0].record(stream)
-        for k in range(args.steps):
-            step(mode, args.warmup + k, dctl[args.warmup + k].data_ptr())
-            evs[k + 1].record(stream)
+        if graph:
+            k = 0
+            for cnt, g in graphs:
+                run.replay(g)
+                k += cnt
+                evs[k].record(stream)
+        else:
+            for k in range(args.steps):
+                run.step(dctl[args.warmup + k].data_ptr(), config)
+                evs[k + 1].record(stream)
         evs[-1].synchronize()
         if clk:
             clk.__exit__()
         barrier()
-        ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
-        t = sum(ms)
-        if dist:
-            tt = torch.tensor([t], device=dev.device)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t, ms
+        if graph:  # one time per graph
+            marks = [0] + list(np.cumsum([cnt for cnt, _ in graphs]))
+            ms = [evs[marks[i]].elapsed_time(evs[marks[i + 1]]) for i in range(len(graphs))]
+        else:
+            ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+        t = evs[0].elapsed_time(evs[-1])
+        del graphs
+        return reduce_max(t), ms
 
-    # ---- the plain one-thread-per-arena launch, then this mode, each from the same start states and controls ----
-    plain = None
-    if args.mode != "plain" and not args.no_plain:
-        t_plain, _ = timed("plain")
-        plain = world_size * n * 8 * args.steps / (t_plain / 1e3)
+    # ---- the learned part: labels from exact decisions (their own controls), then training ----
+    pred_info = None
+    if args.mode == "binned":
+        t0 = time.perf_counter()
+        samples, losses = run.train_predictor(args.seed * 1000 + 500 + rank, decisions=args.train_decisions, epochs=args.epochs)
+        pred_info = {"train_samples": samples, "train_seconds": time.perf_counter() - t0, "last_losses": losses}
+
+    # ---- the autotuner: every candidate on the same 2 decisions from the same start states ----
+    tune_ctl = [torch.from_numpy(rsx.decision_controls(args.seed * 1000 + 700 + rank, d, n).view(np.int32)).to(dev.device) for d in range(2)]
+    torch.cuda.synchronize()
+    if args.mode in ("binned", "lockstep") and not args.no_tune:
+        cands = run.candidates(binning=args.mode == "binned")
+        tuned = run.tune([c.data_ptr() for c in tune_ctl], cands)
+        config = dict(run.config)
+        tune_top = [{"ms": round(ms, 3), **c} for ms, c in tuned[:6]]
+    elif args.mode == "plain":
+        config = {"mode": "plain", "block": args.plain_block}
+        tune_top = None
+    else:
+        config = {"mode": args.mode, "block": args.block, "grid": args.grid or run.sms, "split": args.split, "threshold": args.threshold}
+        tune_top = None
+    if dist:  # every rank runs rank 0's configuration
+        obj = [config]
+        dist.broadcast_object_list(obj, src=0)
+        config = obj[0]
+
+    # ---- timing: the plain launch, the best unbinned lockstep, then the chosen configuration ----
+    modes = {}
+    if not args.no_plain and config["mode"] != "plain":
+        t_plain, _ = timed({"mode": "plain", "block": args.plain_block})
+        modes["plain"] = world_size * n * 8 * args.steps / (t_plain / 1e3)
+    if config["mode"] == "binned" and tune_top:
+        unb = next((c for c in [dict(c) for _, c in tuned] if c["mode"] == "lockstep"), None)
+        if unb:
+            t_unb, _ = timed(unb, graph=not args.no_graph)
+            modes["lockstep_unbinned"] = world_size * n * 8 * args.steps / (t_unb / 1e3)
     clk = Clocks(local)
-    t_ms, ms_steps = timed(args.mode, clk)
+    t_ms, ms_steps = timed(config, graph=not args.no_graph and config["mode"] != "plain", clk=clk)
     value = world_size * n * 8 * args.steps / (t_ms / 1e3)
+    modes[config["mode"]] = value
+    words_tuned = run.snapshot()
+
+    # ---- bit-exactness of the chosen configuration against the plain launch (same decisions, same start states) ----
+    exact = None
+    if not args.no_plain and config["mode"] != "plain":
+        timed({"mode": "plain", "block": args.plain_block})
+        a = torch.equal(run.snapshot(), words_tuned)
+        exact = bool(a)
+
+    # ---- recall / precision of the predictor on the timed decisions ----
+    if pred_info is not None:
+        run.restore(start)
+        Zs, Ys = [], []
+        for s in range(steps):
+            cp = dctl[s].data_ptr()
+            run.step(cp, {"mode": "binned", "block": 448, "grid": run.sms, "split": 1, "threshold": 0.5})
+            Zs.append(run.Z.clone())
+            Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
+        stream.synchronize()
+        m = P.recall_precision(torch.cat(Zs).cpu().numpy(), torch.cat(Ys).cpu().numpy())
+        pred_info["recall_precision_rate"] = {k: [round(float(x), 4) for x in v] for k, v in m.items()}
+        pred_info["eval"] = f"{steps} decisions x {n} arenas (the bench's own decisions), threshold 0.5"
 
     # ---- end to end through the public entry point: pinned host controls in, result words out, every step ----
     pin_ctl = torch.from_numpy(ctl_host.view(np.int32)).pin_memory()
     pin_res = torch.zeros(n, dtype=torch.int32).pin_memory()
     dctl1 = torch.zeros((n, 16), dtype=torch.int32, device=dev.device)
+    run.restore(start)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
-        for s in range(2):
+        for s in range(args.warmup):
             dctl1.copy_(pin_ctl[s], non_blocking=True)
-            step(args.mode, s, dctl1.data_ptr())
-            pin_res.copy_(res, non_blocking=True)
+            run.step(dctl1.data_ptr(), config)
+            pin_res.copy_(run.res, non_blocking=True)
         stream.synchronize()
         barrier()
         e0.record(stream)
         for k in range(args.steps):
             dctl1.copy_(pin_ctl[args.warmup + k], non_blocking=True)
-            step(args.mode, args.warmup + k, dctl1.data_ptr())
-            pin_res.copy_(res, non_blocking=True)
+            run.step(dctl1.data_ptr(), config)
+            pin_res.copy_(run.res, non_blocking=True)
             stream.synchronize()  # the caller reads the step's result words
         e1.record(stream)
         e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([e2e_ms], device=dev.device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = reduce_max(e0.elapsed_time(e1))
     e2e = world_size * n * 8 * args.steps / (e2e_ms / 1e3)
     r = pin_res.numpy().view(np.uint32)
     flags = {"scored": int(((r & 0xFF) != 0).sum()), "overflow": int(((r >> 30) & 1).sum()), "unimplemented": int((r >> 31).sum())}
@@ -311,24 +370,25 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "arena-ticks/s", "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded states and arena mesh)",
-            "config": {"workload": "headline: 65,536 arenas per GPU, mixed states, 7x7 car pairings, one 8-tick decision per step",
-                       "arenas_per_gpu": n, "mode": args.mode, "block": args.block if args.mode == "lockstep" else args.plain_block,
-                       "grid": grid if args.mode == "lockstep" else None, "split": args.split if args.mode == "lockstep" else None,
-                       "l2": "inputs larger than L2 (AoSoA state buffer 730 MB per GPU)", "parallelism": f"replicas x{world_size}"},
+            "config": {"workload": f"headline: {n} arenas per GPU, mixed states, 7x7 car pairings, one 8-tick decision per step",
+                       "arenas_per_gpu": n, **config, "cuda_graphs": (not args.no_graph and config["mode"] != "plain"),
+                       "l2": f"inputs larger than L2 (AoSoA state buffer {rsx.aosoa_words(n) * 4 / 1e6:.0f} MB per GPU)",
+                       "parallelism": f"replicas x{world_size}"},
+            "modes": modes,
+            "speedup_vs_plain": value / modes["plain"] if "plain" in modes else None,
+            "bit_exact_vs_plain": exact,
+            "autotune_top": tune_top,
+            "predictor": pred_info,
             "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * 4},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "plain": None if plain is None else {"value": plain, "unit": "arena-ticks/s", "block": args.plain_block,
-                                                 "what": "one thread per arena, one launch per decision (the reference's sim8 shape)"},
-            "speedup_vs_plain": None if plain is None else value / plain,
-            "gpu_launches": args.steps,
+            "gpu_launches": run.kernels_per_step(config) * args.steps,
             "result_flags": flags,
             "ms_per_step_all": ms_steps,
         }))
     torch.cuda.synchronize()
-    ds.free()
-    dsd.free()
+    run.free()
     if dist:
         dist.destroy_process_group()
 

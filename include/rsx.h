@@ -69,6 +69,8 @@ int rsx_states_free(rsx_states* st);
 int rsx_states_upload(rsx_device* dev, rsx_states* st, const uint32_t* aosoa);     /* rsx_aosoa_words(n) words */
 int rsx_states_download(rsx_device* dev, rsx_states* st, uint32_t* aosoa);         /* synchronises */
 uint32_t* rsx_states_device_ptr(rsx_states* st);
+/* device-to-device copy of `bytes` on a caller stream (snapshots of a state buffer; no counterpart in the reference) */
+int rsx_copy_raw(void* d_dst, const void* d_src, uint64_t bytes, void* stream);
 
 /* ---- the decision (SimDevice::sim8, device.rs:155-168; kernel sim.cu:95-104) ----
  * One decision of every arena in place: 8 ticks with controls[a*2+i] (device memory, 16 words per arena), result[a] the
@@ -129,6 +131,36 @@ int rsx_sim8_persistent_noalloc(uint32_t* d_states, uint32_t n, const void* d_st
  * advance by one decision; the goal state is not kept, so use it on a copy. */
 int rsx_profile_phases_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                            const rsx_controls* d_controls, uint64_t* d_phase_cycles, void* stream);
+
+/* ---- the contact predictor (no counterpart in the reference: the binning it drives is this library's) ----
+ * A 48 -> 128 -> 128 -> 128 -> 6 ReLU MLP (sigmoid outputs) over per-arena features, BF16 weights and activations
+ * with FP32 accumulation, trained on the decision kernels' event-OR labels.  Weights: RSX_PRED_PARAMS FP32 master
+ * values and a BF16 copy (uint16 words) of the same layout: W1[128][48] b1[128] W2[128][128] b2[128] W3[128][128]
+ * b3[128] W4[8][128] b4[8] (rows 6 and 7 of W4 zero).  Labels: bit 0 car 0 - ball, 1 car 1 - ball, 2 car - car,
+ * 3 ball - world, 4 car 0 - world, 5 car 1 - world.  All buffers are device memory; calls are asynchronous. */
+#define RSX_PRED_FEATURES 48
+#define RSX_PRED_LABELS 6
+#define RSX_PRED_PARAMS 40328
+int rsx_pred_features_raw(const uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                          const rsx_controls* d_controls, uint16_t* d_features, void* stream);
+int rsx_pred_labels_raw(const uint32_t* d_event_or, uint32_t n, uint8_t* d_labels, void* stream);
+/* logits[n][8] (FP32; outputs 6, 7 unused) */
+int rsx_pred_forward_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
+                         void* stream);
+/* BF16 elements of the training scratch for a batch of n */
+uint64_t rsx_pred_scratch_elems(uint32_t n);
+/* gradients of L = (1/n) sum over the batch and the 6 outputs of the binary cross-entropy: d_grad[RSX_PRED_PARAMS]
+ * (overwritten), d_loss[0] = n L, d_logits[n][8] the forward's logits */
+int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, const uint8_t* d_labels,
+                           uint32_t n, uint16_t* d_scratch, float* d_logits, float* d_grad, float* d_loss, void* stream);
+/* one Adam step (beta 0.9, 0.999, eps 1e-8) of the FP32 master weights with moments d_m, d_v; refreshes the BF16 copy */
+int rsx_pred_adam_raw(float* d_w_f32, uint16_t* d_w_bf16, float* d_m, float* d_v, const float* d_grad, uint32_t step, float lr,
+                      void* stream);
+int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream);
+/* Bins: arena a is contact-heavy when any of its 6 logits exceeds threshold_logit.  d_order[n] lists the heavy arenas
+ * then the quiet ones, each in arena order; d_heavy_count[0] their number; d_scratch ceil(n / 1024) words. */
+int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t* d_scratch, uint32_t* d_order,
+                     uint32_t* d_heavy_count, void* stream);
 
 /* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
 /* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */

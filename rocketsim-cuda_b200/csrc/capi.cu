@@ -28,6 +28,18 @@ RSX_DECL_PERSIST(16)
 RSX_DECL_LOCKSTEP(384)
 RSX_DECL_LOCKSTEP(448)
 RSX_DECL_LOCKSTEP(512)
+cudaError_t rsx_launch_pred_features(const uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t n,
+                                     void* X, cudaStream_t s);
+cudaError_t rsx_launch_pred_labels(const uint32_t* ev, uint32_t n, uint8_t* Y, cudaStream_t s);
+cudaError_t rsx_launch_pred_forward(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, cudaStream_t s);
+cudaError_t rsx_launch_pred_backward(const void* wb, const float* wf, const float* logits, const uint8_t* Y, const void* save, uint32_t n,
+                                     float inv_scale, void* dz, void* dsave, float* loss_sum, cudaStream_t s);
+cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* save, const void* dsave, uint32_t n, float* grad, cudaStream_t s);
+cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
+                                 float c2, cudaStream_t s);
+cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
+cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t* block_scratch, uint32_t* order, uint32_t* heavy_total,
+                                cudaStream_t s);
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
 cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
 cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
@@ -267,6 +279,80 @@ int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics,
     e = rsx_launch_sim8_lockstep_t512(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
                                       block, (int)split, s);
   RSX_CK(e);
+  return RSX_OK;
+}
+
+int rsx_copy_raw(void* d_dst, const void* d_src, uint64_t bytes, void* stream) {
+  if (!d_dst || !d_src) return RSX_E_ARG;
+  if (bytes == 0) return RSX_OK;
+  RSX_CK(cudaMemcpyAsync(d_dst, d_src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+// ---- the contact predictor ----
+uint64_t rsx_pred_scratch_elems(uint32_t n) { return 2ull * (3ull * n + 16) * 128 + (uint64_t)(n + 16) * 8; }
+
+int rsx_pred_features_raw(const uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                          uint16_t* d_features, void* stream) {
+  if (!d_states || !d_statics || !d_controls || !d_features) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_features(d_states, d_statics, d_sd_index, d_controls, n, d_features, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_labels_raw(const uint32_t* d_event_or, uint32_t n, uint8_t* d_labels, void* stream) {
+  if (!d_event_or || !d_labels) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_labels(d_event_or, n, d_labels, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_forward_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits, void* stream) {
+  if (!d_w_bf16 || !d_w_f32 || !d_features || !d_logits) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_forward(d_w_bf16, d_w_f32, d_features, n, d_logits, nullptr, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, const uint8_t* d_labels, uint32_t n,
+                           uint16_t* d_scratch, float* d_logits, float* d_grad, float* d_loss, void* stream) {
+  if (!d_w_bf16 || !d_w_f32 || !d_features || !d_labels || !d_scratch || !d_logits || !d_grad || !d_loss || n == 0) return RSX_E_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  uint16_t* save = d_scratch;
+  uint16_t* dsave = save + (3ull * n + 16) * 128;
+  uint16_t* dz = dsave + (3ull * n + 16) * 128;
+  RSX_CK(cudaMemsetAsync(d_grad, 0, RSX_PRED_PARAMS * sizeof(float), s));
+  RSX_CK(cudaMemsetAsync(d_loss, 0, sizeof(float), s));
+  RSX_CK(cudaMemsetAsync(save + 3ull * n * 128, 0, 16 * 128 * 2, s));  // the rows past n that the last tile reads
+  RSX_CK(rsx_launch_pred_forward(d_w_bf16, d_w_f32, d_features, n, d_logits, save, s));
+  RSX_CK(rsx_launch_pred_backward(d_w_bf16, d_w_f32, d_logits, d_labels, save, n, 1.0f / (float)n, dz, dsave, d_loss, s));
+  RSX_CK(rsx_launch_pred_wgrads(d_features, dz, save, dsave, n, d_grad, s));
+  return RSX_OK;
+}
+
+int rsx_pred_adam_raw(float* d_w_f32, uint16_t* d_w_bf16, float* d_m, float* d_v, const float* d_grad, uint32_t step, float lr, void* stream) {
+  if (!d_w_f32 || !d_w_bf16 || !d_m || !d_v || !d_grad || step == 0) return RSX_E_ARG;
+  const float b1 = 0.9f, b2 = 0.999f;
+  float p1 = 1.0f, p2 = 1.0f;
+  for (uint32_t i = 0; i < step && i < 100000u; ++i) {
+    p1 *= b1;
+    p2 *= b2;
+  }
+  RSX_CK(rsx_launch_pred_adam(d_w_f32, d_w_bf16, d_m, d_v, d_grad, lr, b1, b2, 1e-8f, 1.0f - p1, 1.0f - p2, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream) {
+  if (!d_w_f32 || !d_w_bf16) return RSX_E_ARG;
+  RSX_CK(rsx_launch_pred_to_bf16(d_w_f32, d_w_bf16, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t* d_scratch, uint32_t* d_order, uint32_t* d_heavy_count,
+                     void* stream) {
+  if (!d_logits || !d_scratch || !d_order || !d_heavy_count) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_bin(d_logits, n, threshold_logit, d_scratch, d_order, d_heavy_count, (cudaStream_t)stream));
   return RSX_OK;
 }
 

@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
                                               ctypes.c_uint32, vp]
         L.rsx_sim8_lockstep_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, vp]
+        L.rsx_copy_raw.argtypes = [vp, vp, ctypes.c_uint64, vp]
         _lib = L
     return _lib
 

@@ -1,0 +1,178 @@
+"""Batched decisions on one GPU: the decision kernels, the learned binning in front of them, CUDA-graph capture of many
+decisions, and the autotuner that picks the launch configuration.
+
+A `DecisionRunner` owns the device buffers of one batch of arenas (AoSoA-32 states, per-arena car pairing, results,
+event words, queue counter, arena order, predictor features and logits) and issues one decision with `step()`:
+
+  plain     k_sim8_multi, one thread per arena, one launch per decision (the reference's sim8 shape, block 32)
+  lockstep  the SM-lockstep persistent kernel (rsx_sim8_lockstep_raw) over the identity order
+  binned    the same kernel over the contact predictor's order: features -> MLP -> heavy/quiet bins -> order
+
+Every configuration computes the same words (no cross-arena arithmetic), so the autotuner may pick any of them by
+time alone; `tune()` restores the same start states before each candidate so that all candidates step identical work.
+"""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+
+import rsx
+import predictor as P
+
+
+class DecisionRunner:
+    def __init__(self, dev: "rsx.SimDevice", statics: np.ndarray, sd_index: np.ndarray, states: np.ndarray, stream=None):
+        import torch
+
+        self.torch = torch
+        self.dev = dev
+        self.n = states.shape[0]
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=dev.device)
+        self.sptr = self.stream.cuda_stream
+        self.dsd = dev.upload_static(statics)
+        self.ds = dev.upload_states(states)
+        n = self.n
+        t = torch
+        self.didx = t.from_numpy(np.ascontiguousarray(sd_index, dtype=np.uint8)).to(dev.device)
+        self.res = t.zeros(n, dtype=t.int32, device=dev.device)
+        self.ev = t.zeros(n, dtype=t.int32, device=dev.device)
+        self.counter = t.zeros(1, dtype=t.int32, device=dev.device)
+        self.order = t.zeros(n, dtype=t.int32, device=dev.device)
+        self.heavy = t.zeros(1, dtype=t.int32, device=dev.device)
+        self.bin_scratch = t.zeros((n + 1023) // 1024, dtype=t.int32, device=dev.device)
+        self.X = t.zeros((n, P.FEATURES), dtype=t.int16, device=dev.device)
+        self.Z = t.zeros((n, 8), dtype=t.float32, device=dev.device)
+        self.sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
+        self.pred = None
+        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 1, "threshold": None}
+        torch.cuda.synchronize(dev.device)
+
+    # ---- one decision ----
+    def step(self, controls_ptr: int, config: dict | None = None) -> None:
+        c = config or self.config
+        L = rsx.lib()
+        n = self.n
+        if c["mode"] == "plain":
+            rsx.check(L.rsx_sim8_multi_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
+                                           self.ev.data_ptr(), c.get("block", 32), self.sptr), "rsx_sim8_multi_raw")
+            return
+        order = None
+        if c["mode"] == "binned":
+            p = self.pred
+            thr = float(np.log(c["threshold"] / (1.0 - c["threshold"])))
+            rsx.check(p.L.rsx_pred_features_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.X.data_ptr(),
+                                                self.sptr), "features")
+            rsx.check(p.L.rsx_pred_forward_raw(p.wb.data_ptr(), p.w.data_ptr(), self.X.data_ptr(), n, self.Z.data_ptr(), self.sptr),
+                      "forward")
+            rsx.check(p.L.rsx_pred_bin_raw(self.Z.data_ptr(), n, thr, self.bin_scratch.data_ptr(), self.order.data_ptr(),
+                                           self.heavy.data_ptr(), self.sptr), "bin")
+            order = self.order.data_ptr()
+        rsx.check(L.rsx_sim8_lockstep_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
+                                          self.ev.data_ptr(), order, self.counter.data_ptr(), c.get("grid", self.sms), c["block"],
+                                          c["split"], self.sptr), "rsx_sim8_lockstep_raw")
+
+    def kernels_per_step(self, config: dict | None = None) -> int:
+        """This library's kernel launches per decision (features, forward, two binning passes, the decision)."""
+        c = config or self.config
+        return 5 if c["mode"] == "binned" else 1
+
+    # ---- states ----
+    def snapshot(self):
+        """A device copy of the states (restored by restore())."""
+        t = self.torch
+        words = rsx.aosoa_words(self.n)
+        buf = t.empty(words, dtype=t.int32, device=self.dev.device)
+        rsx.check(rsx.lib().rsx_copy_raw(buf.data_ptr(), self.ds.ptr(), words * 4, self.sptr), "rsx_copy_raw")
+        self.stream.synchronize()  # the copy is complete for readers on any stream
+        return buf
+
+    def restore(self, buf) -> None:
+        rsx.check(rsx.lib().rsx_copy_raw(self.ds.ptr(), buf.data_ptr(), rsx.aosoa_words(self.n) * 4, self.sptr), "rsx_copy_raw")
+
+    # ---- the learned part ----
+    def train_predictor(self, control_seed: int, decisions: int = 32, epochs: int = 3, seed: int = 0, lr: float = 1e-3):
+        """Labels from `decisions` exact decisions of these arenas (controls of `control_seed`, run on a snapshot that is
+        restored afterwards), then Adam over them; returns (samples, last losses)."""
+        t = self.torch
+        if self.pred is None:
+            self.pred = P.ContactPredictor(self.dev.device, seed=seed, stream=self.sptr)
+        snap = self.snapshot()
+        Xs, Ys = [], []
+        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 1}
+        for d in range(decisions):
+            ctl = t.from_numpy(rsx.decision_controls(control_seed, d, self.n).view(np.int32)).to(self.dev.device, non_blocking=False)
+            self.stream.wait_stream(t.cuda.current_stream(self.dev.device))
+            X = t.empty((self.n, P.FEATURES), dtype=t.int16, device=self.dev.device)
+            Y = t.empty(self.n, dtype=t.uint8, device=self.dev.device)
+            rsx.check(self.pred.L.rsx_pred_features_raw(self.ds.ptr(), self.n, self.dsd.ptr(), self.didx.data_ptr(), ctl.data_ptr(),
+                                                        X.data_ptr(), self.sptr), "features")
+            self.step(ctl.data_ptr(), cfg)
+            rsx.check(self.pred.L.rsx_pred_labels_raw(self.ev.data_ptr(), self.n, Y.data_ptr(), self.sptr), "labels")
+            self.stream.synchronize()
+            Xs.append(X)
+            Ys.append(Y)
+        self.restore(snap)
+        self.stream.synchronize()
+        X, Y = t.cat(Xs), t.cat(Ys)
+        with t.cuda.stream(self.stream):
+            losses = []
+            for ep in range(epochs):
+                losses = self.pred.fit(X, Y, epochs=1, batch=8192, lr=lr, seed=seed + ep)
+        self.stream.synchronize()
+        return X.shape[0], losses
+
+    # ---- the autotuner ----
+    def candidates(self, binning: bool = True):
+        out = []
+        for block, split in itertools.product((384, 448, 512), (0, 1)):
+            out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
+            if binning and self.pred is not None:
+                for thr in (0.3, 0.5):
+                    out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr})
+        return out
+
+    def tune(self, controls_ptrs, candidates=None, repeats: int = 1):
+        """Times every candidate on the same decisions from the same start states; keeps the fastest as self.config.
+        Returns [(ms, config)] sorted by time."""
+        t = self.torch
+        snap = self.snapshot()
+        results = []
+        for c in candidates or self.candidates():
+            best = None
+            for _ in range(repeats):
+                self.restore(snap)
+                e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+                e0.record(self.stream)
+                for cp in controls_ptrs:
+                    self.step(cp, c)
+                e1.record(self.stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            results.append((best, c))
+        self.restore(snap)
+        self.stream.synchronize()
+        results.sort(key=lambda r: r[0])
+        self.config = dict(results[0][1])
+        return results
+
+    # ---- CUDA graphs ----
+    def capture(self, controls_ptrs, config: dict | None = None):
+        """One CUDA graph of len(controls_ptrs) consecutive decisions (each with its own controls buffer)."""
+        t = self.torch
+        g = t.cuda.CUDAGraph()
+        self.stream.synchronize()
+        with t.cuda.graph(g, stream=self.stream):
+            for cp in controls_ptrs:
+                self.step(cp, config)
+        return g
+
+    def replay(self, g) -> None:
+        """Replays a captured graph on this runner's stream (torch replays on the current stream)."""
+        with self.torch.cuda.stream(self.stream):
+            g.replay()
+
+    def free(self):
+        self.ds.free()
+        self.dsd.free()
