@@ -5,8 +5,9 @@
 // into different phases, every warp's instruction fetches evict the others' and the SM stalls on instruction misses
 // (measured on the one-thread-per-arena launch: ~26 cycles of "no instruction" stall per issued instruction, issue
 // active 4% of cycles).  Here the warps of a block step their arenas phase by phase together: a __syncthreads()
-// after each of the ten phases (and, with `split`, after each car's pre-tick inside P1), so that at any time the
-// block's warps fetch from one phase's code.
+// after each of the ten phases (split 1: also after each car's pre-tick inside P1; split 2: P1 of each car in three
+// parts, pre-tick head / wheel rays / wheel response), so that at any time the block's warps fetch from one piece of
+// code.
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -67,7 +68,42 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
       s.cars[0].controls = c0;
       s.cars[1].controls = c1;
     }
-    if (SPLIT) {
+    if (SPLIT == 2) {
+      if (have) sim::t_p0(s, *D);
+      __syncthreads();
+      if (have) {
+        sim::flip_zdamp(s, *D, 0);
+        sim::flip_zdamp(s, *D, 1);
+      }
+#pragma unroll 1
+      for (int ci = 0; ci < kCars; ++ci) {
+        // P1 for car ci in three barrier-separated parts: pre-tick head, wheel rays, wheel response + tail
+        bool act = false;
+        float rthr = 0.0f;
+        uint32_t was = 0;
+        if (have) {
+          was = s.cars[ci].on_ground;
+          act = sim::car_pre_tick_head(s, *D, ci, &rthr);
+        }
+        __syncthreads();
+        sim::WheelHit hits[kWheels];
+        if (have && act) sim::vehicle_rays(s, *D, ci, hits);
+        __syncthreads();
+        if (have) {
+          if (act) {
+            sim::vehicle_response(s, *D, ci, sim::kTickTime, s.cars[ci].handbrake_val, rthr, D->cars[ci].three_wheels != 0, hits);
+            sim::car_pre_tick_tail(s, *D, ci);
+          }
+          if (!was && s.cars[ci].on_ground) s.events |= 1u << (EV_LANDED + ci);
+        }
+        __syncthreads();
+      }
+#pragma unroll 1
+      for (int k = 2; k < sim::kPhases; ++k) {
+        if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
+        __syncthreads();
+      }
+    } else if (SPLIT) {
       if (have) sim::t_p0(s, *D);
       __syncthreads();
       if (have) {
@@ -126,7 +162,9 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
                    const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split)
+  if (split == 2)
+    K_NAME<2><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split)
     K_NAME<1><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
   else
     K_NAME<0><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);

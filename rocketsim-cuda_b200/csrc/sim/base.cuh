@@ -7,6 +7,31 @@
 #include "../state.cuh"
 #include "../crmath.cuh"
 
+// Zone timers of profiling builds (RSX_ZONES defined, device code): the lowest active lane of each group of lanes that
+// runs a zone adds the zone's clock cycles to its warp's slot rsx_zone_acc[warp][id], so the sums are warp cycles spent in each
+// zone.  The including translation unit defines rsx_zone_acc.  Without RSX_ZONES the markers are empty.
+#if defined(RSX_ZONES) && defined(__CUDA_ARCH__)
+#ifndef RSX_ZONES_MIN
+#define RSX_ZONES_MIN 0
+#endif
+extern __device__ unsigned long long rsx_zone_acc[148 * 16][64];
+#define RSX_ZONE_BEGIN(v) long long v = clock64()
+#define RSX_ZONE_END(v, id)                                                                              \
+  do {                                                                                                   \
+    unsigned m_ = __activemask();                                                                        \
+    if ((id) >= RSX_ZONES_MIN && (threadIdx.x & 31u) == (unsigned)(__ffs(m_) - 1))                      \
+      atomicAdd(&rsx_zone_acc[(blockIdx.x * 16u + (threadIdx.x >> 5)) % (148u * 16u)][id],               \
+                (unsigned long long)(clock64() - v));                                                    \
+  } while (0)
+#else
+#define RSX_ZONE_BEGIN(v) \
+  do {                    \
+  } while (0)
+#define RSX_ZONE_END(v, id) \
+  do {                      \
+  } while (0)
+#endif
+
 namespace rsx {
 namespace sim {
 

@@ -159,43 +159,69 @@ RSX_F void update_axis(ArenaState& S, const StaticData& D, int axis, uint32_t h,
 }
 
 // ---- the ray grid's dynamic entries: sorted by cell, list order within a cell ----
-RSX_F void dyn_cell_push(ArenaState& S, uint32_t cell, uint32_t h) {
-  if (S.n_dyn_cells >= (uint32_t)kMaxDynCells) {
-    S.overflow[OVF_DYN_CELLS] += 1;
-    return;
-  }
-  uint32_t at = 0;
-  while (at < S.n_dyn_cells && S.dyn_cells[at].cell <= cell) ++at;
-  for (uint32_t i = S.n_dyn_cells; i > at; --i) S.dyn_cells[i] = S.dyn_cells[i - 1];
-  S.dyn_cells[at] = DynCell{cell, h};
-  S.n_dyn_cells += 1;
-}
-RSX_F void dyn_cell_remove(ArenaState& S, uint32_t cell, uint32_t h) {
-  for (uint32_t at = 0; at < S.n_dyn_cells; ++at) {
-    if (S.dyn_cells[at].cell == cell && S.dyn_cells[at].handle == h) {
-      for (uint32_t i = at; i + 1 < S.n_dyn_cells; ++i) S.dyn_cells[i] = S.dyn_cells[i + 1];
-      S.dyn_cells[S.n_dyn_cells - 1] = DynCell{0, 0};
-      S.n_dyn_cells -= 1;
-      return;
-    }
-  }
-}
-RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_t h, const uint32_t idx[3]) {
-  uint32_t lo[3], hi[3];
+// A body moving to another cell leaves the 3x3x3 block of cells around its old cell and enters the block around its new
+// one.  The reference does this cell by cell: a removal finds the first (cell, handle) entry, shifts the tail left and
+// zeroes the freed last slot; an insertion (skipped, counting an overflow, when the list is full) goes after every entry
+// of a lower or equal cell.  The two passes below give the same list, the same zeroed slots and the same overflow
+// count in one sweep each: removal keeps every entry but the first of each block cell for the handle, then zeroes the
+// freed slots; insertion merges the block's cells (ascending, the first ones that fit) after equal cells, from the back.
+RSX_F void dyn_block_range(const StaticData& D, const uint32_t idx[3], uint32_t lo[3], uint32_t hi[3]) {
   for (int a = 0; a < 3; ++a) {
     uint32_t m = idx[a] > 1 ? idx[a] : 1;
     lo[a] = m - 1;
     uint32_t top = D.grid_n[a] - 1, p = idx[a] + 1;
     hi[a] = top < p ? top : p;
   }
+}
+RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_t h, const uint32_t idx[3]) {
+  uint32_t lo[3], hi[3];
+  dyn_block_range(D, idx, lo, hi);
+  const uint32_t ny = D.grid_n[1], nz = D.grid_n[2];
+  if (!add) {
+    uint32_t removed = 0;  // bit (i - lo0) * 9 + (j - lo1) * 3 + (k - lo2): that cell's entry is gone
+    uint32_t n = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells, w = 0;
+    for (uint32_t r = 0; r < n; ++r) {
+      DynCell e = S.dyn_cells[r];
+      if (e.handle == h) {
+        uint32_t i = e.cell / (ny * nz), j = (e.cell / nz) % ny, k = e.cell % nz;
+        if (i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
+          uint32_t bit = 1u << ((i - lo[0]) * 9 + (j - lo[1]) * 3 + (k - lo[2]));
+          if (!(removed & bit)) {
+            removed |= bit;
+            continue;
+          }
+        }
+      }
+      if (w != r) S.dyn_cells[w] = e;
+      ++w;
+    }
+    for (uint32_t r = w; r < n; ++r) S.dyn_cells[r] = DynCell{0, 0};
+    S.n_dyn_cells = w;
+    return;
+  }
+  uint32_t cells[27];
+  uint32_t nb = 0;
   for (uint32_t i = lo[0]; i <= hi[0]; ++i)
     for (uint32_t j = lo[1]; j <= hi[1]; ++j)
       for (uint32_t k = lo[2]; k <= hi[2]; ++k) {
         uint32_t c3[3] = {i, j, k};
-        uint32_t cell = cell_of(D, c3);
-        if (add) dyn_cell_push(S, cell, h);
-        else dyn_cell_remove(S, cell, h);
+        cells[nb++] = cell_of(D, c3);
       }
+  uint32_t n = S.n_dyn_cells;
+  uint32_t room = n < (uint32_t)kMaxDynCells ? (uint32_t)kMaxDynCells - n : 0u;
+  uint32_t take = nb < room ? nb : room;
+  S.overflow[OVF_DYN_CELLS] += nb - take;
+  if (take == 0) return;
+  int32_t ia = (int32_t)n - 1, ib = (int32_t)take - 1, out = (int32_t)(n + take) - 1;
+  while (ib >= 0) {
+    if (ia >= 0 && S.dyn_cells[ia].cell > cells[ib]) {
+      S.dyn_cells[out--] = S.dyn_cells[ia--];
+    } else {
+      S.dyn_cells[out--] = DynCell{cells[ib], h};
+      --ib;
+    }
+  }
+  S.n_dyn_cells = n + take;
 }
 
 RSX_F Box3 dyn_shape_box(const BodyConst& c, const Aff& t) {

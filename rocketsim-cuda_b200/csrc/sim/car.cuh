@@ -220,15 +220,12 @@ RSX_F V3 steered_axle(const Aff& cxf, float angle) {
   return qrotate(quat_axis_sc(cxf.m.c2, s, c), cxf.m.c1);
 }
 
-RSX_HD RSX_NOINL inline void vehicle_update(ArenaState& S, const StaticData& D, int ci, float dt, float hb, float thr, bool three) {
+// the wheels' hard points and the four wheel rays against the world (the first half of vehicle_update)
+RSX_HD RSX_NOINL inline void vehicle_rays(ArenaState& S, const StaticData& D, int ci, WheelHit hits[kWheels]) {
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   const uint32_t cidx = cc.body;
-  const int cd = slot(D, cidx);
-  const BodyConst& cbc = D.bodies[cidx];
-  Aff cxf = S.bodies[cd].xf;
-  V3 ct = cxf.t;
-  float fscale = fdiv(mass_of(cbc), 3.0f);
+  Aff cxf = S.bodies[slot(D, cidx)].xf;
   V3 src[kWheels], tgt[kWheels];
   for (int i = 0; i < kWheels; ++i) {
     Wheel& w = car.wheels[i];
@@ -237,8 +234,23 @@ RSX_HD RSX_NOINL inline void vehicle_update(ArenaState& S, const StaticData& D, 
     tgt[i] = w.hard_point - (cxf.m.c2 * wc.ray_length);
     src[i] = w.hard_point;
   }
-  WheelHit hits[kWheels];
+  RSX_ZONE_BEGIN(z_rays);
   cast_wheel_rays(S, D, src, tgt, cidx, hits);
+  RSX_ZONE_END(z_rays, 1);
+}
+
+// the wheels' response to the ray hits: suspension, friction and their impulses (the second half of vehicle_update)
+RSX_HD RSX_NOINL inline void vehicle_response(ArenaState& S, const StaticData& D, int ci, float dt, float hb, float thr, bool three,
+                                              const WheelHit hits[kWheels]) {
+  Car& car = S.cars[ci];
+  const CarConst& cc = D.cars[ci];
+  const uint32_t cidx = cc.body;
+  const int cd = slot(D, cidx);
+  const BodyConst& cbc = D.bodies[cidx];
+  Aff cxf = S.bodies[cd].xf;
+  V3 ct = cxf.t;
+  float fscale = fdiv(mass_of(cbc), 3.0f);
+  RSX_ZONE_BEGIN(z_resp);
   bool have_axle = false;
   float axle_angle = 0.0f;
   V3 axle = vzero();
@@ -338,6 +350,14 @@ RSX_HD RSX_NOINL inline void vehicle_update(ArenaState& S, const StaticData& D, 
     V3 rel = off - cxf.m.c2 * upd;
     add_impulse(S.bodies[cd], cbc, IMP_LINEAR_AT, ri.impulse * dt, rel, true, false);
   }
+  RSX_ZONE_END(z_resp, 2);
+}
+
+// vehicle_rl.cuh:56-138: rays, then the response (the rays read body poses only; the response writes velocities)
+RSX_F void vehicle_update(ArenaState& S, const StaticData& D, int ci, float dt, float hb, float thr, bool three) {
+  WheelHit hits[kWheels];
+  vehicle_rays(S, D, ci, hits);
+  vehicle_response(S, D, ci, dt, hb, thr, three, hits);
 }
 
 // ---- the car's pre-tick ----
@@ -629,7 +649,10 @@ RSX_F void flip_zdamp(ArenaState& S, const StaticData& D, int ci) {
   if (rb.lin_vel.z < 0.0f || car.flip_time < kFlipZDampEnd) rb.lin_vel.z = fmul(rb.lin_vel.z, fsub(1.0f, kFlipZDamp120));
 }
 
-RSX_F void car_pre_tick(ArenaState& S, const StaticData& D, int ci) {
+// The car's pre-tick up to its vehicle update; false for a demolished car (whose pre-tick ends here).  *rthr receives the
+// throttle the vehicle update uses.
+RSX_F bool car_pre_tick_head(ArenaState& S, const StaticData& D, int ci, float* rthr_out) {
+  RSX_ZONE_BEGIN(z_pre);
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   Body& rb = S.bodies[slot(D, cc.body)];
@@ -638,7 +661,7 @@ RSX_F void car_pre_tick(ArenaState& S, const StaticData& D, int ci) {
     if (car.demo_respawn_timer == 0.0f) respawn(S, D, ci, D.mut[M_SPAWN_BOOST]);
     if (rb.activation != ACT_DISABLED) rb.activation = ACT_DISABLED;
     rb.flags |= CF_NO_RESPONSE;
-    return;
+    return false;
   }
   force_activate(rb);
   rb.flags &= ~CF_NO_RESPONSE;
@@ -668,13 +691,29 @@ RSX_F void car_pre_tick(ArenaState& S, const StaticData& D, int ci) {
     update_auto_roll(S, D, ci, rb, nwic, uc);
   car.world_contact_normal = Opt<V3>{};
   update_boost(S, D, ci, rb);
-  float rthr = (car.controls.boost && car.boost > 0.0f) ? 1.0f : qthr;
-  vehicle_update(S, D, ci, kTickTime, car.handbrake_val, rthr, cc.three_wheels != 0);
+  *rthr_out = (car.controls.boost && car.boost > 0.0f) ? 1.0f : qthr;
+  RSX_ZONE_END(z_pre, 0);
+  return true;
+}
+
+// the car's pre-tick after its vehicle update: wheel contact state and the sticky-force gate
+RSX_F void car_pre_tick_tail(ArenaState& S, const StaticData& D, int ci) {
+  Car& car = S.cars[ci];
+  RSX_ZONE_BEGIN(z_post);
   update_contact_state(S, D, ci);
   uint32_t world = 0;
   for (int i = 0; i < kWheels; ++i)
     if (car.wheels[i].ray.some && car.wheels[i].ray.v.in_contact_with_world) world = 1;
   car.sticky_gate_prev = world;
+  RSX_ZONE_END(z_post, 3);
+}
+
+// car_pre_tick.cuh:638-705
+RSX_F void car_pre_tick(ArenaState& S, const StaticData& D, int ci) {
+  float rthr;
+  if (!car_pre_tick_head(S, D, ci, &rthr)) return;
+  vehicle_update(S, D, ci, kTickTime, S.cars[ci].handbrake_val, rthr, D.cars[ci].three_wheels != 0);
+  car_pre_tick_tail(S, D, ci);
 }
 
 RSX_F void phase1(ArenaState& S, const StaticData& D) {

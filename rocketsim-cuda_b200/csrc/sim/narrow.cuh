@@ -935,7 +935,10 @@ RSX_F int near_head(Ctx& c, uint32_t rb0, uint32_t rb1, NearPair& np, BoxJob& bj
     int32_t pi = cached;
     if (pi < 0) pi = insert_manifold(S, manifold_new(cv, cc));
     if (pi < 0) return NEAR_DONE;
-    if (sphere_job_begin(c, cv, cc, pi, sj)) return NEAR_SPHERE_JOB;
+    RSX_ZONE_BEGIN(z_sj);
+    bool job = sphere_job_begin(c, cv, cc, pi, sj);
+    RSX_ZONE_END(z_sj, 21);
+    if (job) return NEAR_SPHERE_JOB;
     push_active(S, (uint32_t)pi);
     return NEAR_DONE;
   }
@@ -943,22 +946,38 @@ RSX_F int near_head(Ctx& c, uint32_t rb0, uint32_t rb1, NearPair& np, BoxJob& bj
   bool has = false;
   uint32_t ko = c.D.bodies[other].shape;
   if (cpair && (ko == SHAPE_PLANE || ko == SHAPE_MESH)) {
-    if (ko == SHAPE_PLANE) has = alg_convex_plane(c, comp_i, other, child_xf(S, c.D, comp_i), true, &fresh);
-    else if (box_job_begin(c, comp_i, other, bj)) return NEAR_BOX_JOB;
+    if (ko == SHAPE_PLANE) {
+      RSX_ZONE_BEGIN(z_cp);
+      has = alg_convex_plane(c, comp_i, other, child_xf(S, c.D, comp_i), true, &fresh);
+      RSX_ZONE_END(z_cp, 17);
+    } else {
+      RSX_ZONE_BEGIN(z_bj);
+      bool job = box_job_begin(c, comp_i, other, bj);
+      RSX_ZONE_END(z_bj, 22);
+      if (job) return NEAR_BOX_JOB;
+    }
   } else if (k0 == SHAPE_PLANE && k1 == SHAPE_SPHERE) {
     has = alg_convex_plane(c, rb1, rb0, body_xf(S, c.D, rb1), false, &fresh);
   } else if (k0 == SHAPE_SPHERE && k1 == SHAPE_PLANE) {
     has = alg_convex_plane(c, rb0, rb1, body_xf(S, c.D, rb0), false, &fresh);
   } else if (k0 == SHAPE_SPHERE && k1 == SHAPE_BOX) {
+    RSX_ZONE_BEGIN(z_sb);
     has = alg_sphere_box(c, rb0, rb1, &fresh);
+    RSX_ZONE_END(z_sb, 18);
   } else if (k0 == SHAPE_BOX && k1 == SHAPE_SPHERE) {
+    RSX_ZONE_BEGIN(z_sb);
     has = alg_sphere_box(c, rb1, rb0, &fresh);
+    RSX_ZONE_END(z_sb, 18);
   } else if (k0 == SHAPE_BOX && k1 == SHAPE_BOX) {
+    RSX_ZONE_BEGIN(z_bb);
     has = alg_box_box(c, rb0, rb1, &fresh);
+    RSX_ZONE_END(z_bb, 19);
   } else {
     c.unimplemented += 1;
   }
+  RSX_ZONE_BEGIN(z_nt);
   near_tail(c, rb0, rb1, cached, has, fresh);
+  RSX_ZONE_END(z_nt, 23);
   return NEAR_DONE;
 }
 
@@ -973,16 +992,22 @@ RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {
   SphereJob sj;
   while (kind != NEAR_DONE || i < n) {
     if (kind == NEAR_DONE) {
+      RSX_ZONE_BEGIN(z_head);
       while (i < n) {
         Pair p = S.pairs[i++];
         kind = near_head(c, D.proxies[p.h0].body, D.proxies[p.h1].body, np, bj, sj);
         if (kind != NEAR_DONE) break;
       }
+      RSX_ZONE_END(z_head, 10);
       if (kind == NEAR_DONE) break;
     }
     uint32_t tri;
     if (kind == NEAR_BOX_JOB) {
-      if (box_job_next(D, bj, &tri)) {
+      RSX_ZONE_BEGIN(z_bnext);
+      bool more = box_job_next(D, bj, &tri);
+      RSX_ZONE_END(z_bnext, 12);
+      if (more) {
+        RSX_ZONE_BEGIN(z_sat);
         const Tri& t = D.tris[bj.mesh->tri_first + tri];
         V3 q[3] = {xform_point(bj.mesh_to_box, t.p0), xform_point(bj.mesh_to_box, t.p1), xform_point(bj.mesh_to_box, t.p2)};
         SatHit h;
@@ -993,7 +1018,9 @@ RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {
           }
           add_contact(c, bj.m, bj.car, bj.mesh_body, bj.tri_rot * t.n, h.point_world, h.distance, (int32_t)tri);
         }
+        RSX_ZONE_END(z_sat, 11);
       } else {
+        RSX_ZONE_BEGIN(z_btail);
         Manifold fresh = {};
         bool has = false;
         if (bj.has_m) {
@@ -1005,17 +1032,25 @@ RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {
         }
         near_tail(c, np.rb0, np.rb1, np.cached, has, fresh);
         kind = NEAR_DONE;
+        RSX_ZONE_END(z_btail, 13);
       }
     } else {
-      if (cursor_next(sj.cu, D, *sj.mesh, sj.box, &tri)) {
+      RSX_ZONE_BEGIN(z_snext);
+      bool more = cursor_next(sj.cu, D, *sj.mesh, sj.box, &tri);
+      RSX_ZONE_END(z_snext, 14);
+      if (more) {
+        RSX_ZONE_BEGIN(z_stri);
         SphereTriHit h;
         if (sphere_triangle(D.tris[sj.mesh->tri_first + tri], sj.center, sj.radius, sj.rt, sj.rt2, &h))
           add_contact(c, S.manifolds[sj.manifold], sj.sph, sj.mesh_body, h.normal, h.point + sj.mesh_t, h.depth, (int32_t)tri);
+        RSX_ZONE_END(z_stri, 15);
       } else {
+        RSX_ZONE_BEGIN(z_stail);
         Manifold& m = S.manifolds[sj.manifold];
         if (m.n != 0) refresh_points(S, D, m, sj.sph, sj.mesh_body);
         push_active(S, (uint32_t)sj.manifold);
         kind = NEAR_DONE;
+        RSX_ZONE_END(z_stail, 16);
       }
     }
   }

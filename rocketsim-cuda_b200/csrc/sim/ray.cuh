@@ -384,6 +384,7 @@ RSX_F void ray_box(const BodyConst& bc, LocalRays* lr, const RayBox& rb) {
 
 // ---- one candidate body (collision_world quad_ray_test) ----
 RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk) {
+  RSX_ZONE_BEGIN(z_setup);
   View co = view(S, D, w);
   const BodyConst& bc = D.bodies[w];
   V3 fl[4], tl[4];
@@ -411,14 +412,22 @@ RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, 
   RayBox rb;
   raybox_init(rb, fl, tl);
   for (int i = 0; i < 4; ++i) rb.lmax[i] = lr.frac[i];
-  if (bc.shape == SHAPE_BOX) ray_box(bc, &lr, rb);
-  else if (bc.shape == SHAPE_SPHERE) ray_sphere(bc.sphere_margin, &lr, rb);
-  else if (bc.shape == SHAPE_PLANE) {
+  RSX_ZONE_END(z_setup, 28);
+  RSX_ZONE_BEGIN(z_shape);
+  if (bc.shape == SHAPE_BOX) {
+    ray_box(bc, &lr, rb);
+    RSX_ZONE_END(z_shape, 24);
+  } else if (bc.shape == SHAPE_SPHERE) {
+    ray_sphere(bc.sphere_margin, &lr, rb);
+    RSX_ZONE_END(z_shape, 25);
+  } else if (bc.shape == SHAPE_PLANE) {
     for (int p = 0; p < kPlanes; ++p)
       if (D.planes[p].body == w) ray_plane(D.planes[p], &lr, rb);
+    RSX_ZONE_END(z_shape, 26);
   } else {
     for (int m = 0; m < kMeshes; ++m)
       if (D.meshes[m].body == w) ray_mesh(D, D.meshes[m], &lr, &rb);
+    RSX_ZONE_END(z_shape, 27);
   }
 }
 
