@@ -6,8 +6,8 @@
 // (measured on the one-thread-per-arena launch: ~26 cycles of "no instruction" stall per issued instruction, issue
 // active 4% of cycles).  Here the warps of a block step their arenas phase by phase together: a __syncthreads()
 // after each of the ten phases (split 1: also after each car's pre-tick inside P1; split 2: P1 of each car in three
-// parts, pre-tick head / wheel rays / wheel response), so that at any time the block's warps fetch from one piece of
-// code.
+// parts, pre-tick head / wheel rays / wheel response; split 3: also a barrier after every step of P3b's pair / leaf
+// loop), so that at any time the block's warps fetch from one piece of code.
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
       s.cars[0].controls = c0;
       s.cars[1].controls = c1;
     }
-    if (SPLIT == 2) {
+    if (SPLIT >= 2) {
       if (have) sim::t_p0(s, *D);
       __syncthreads();
       if (have) {
@@ -100,6 +100,16 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
       }
 #pragma unroll 1
       for (int k = 2; k < sim::kPhases; ++k) {
+        if (SPLIT == 3 && k == 4) {
+          // P3b with a barrier after every step of the pair / leaf loop
+          sim::P3bLoop L;
+          bool more = have;
+          if (have) sim::p3b_begin(s, L);
+          while (__syncthreads_or(more))
+            if (more) more = sim::t_p3b_step(s, *D, L);
+          if (have && L.unimplemented != 0) un = 1;
+          continue;
+        }
         if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
         __syncthreads();
       }
@@ -162,7 +172,9 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
                    const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split == 2)
+  if (split == 3)
+    K_NAME<3><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 2)
     K_NAME<2><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
   else if (split)
     K_NAME<1><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);

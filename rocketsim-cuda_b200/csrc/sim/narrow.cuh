@@ -981,80 +981,105 @@ RSX_F int near_head(Ctx& c, uint32_t rb0, uint32_t rb1, NearPair& np, BoxJob& bj
   return NEAR_DONE;
 }
 
-// P3b driver: pairs in order; a mesh pair's leaves one by one, each leaf's contact added in order.
-RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {
-  Ctx c = {S, D, 0};
-  uint32_t n = S.n_pairs < (uint32_t)kMaxPairs ? S.n_pairs : (uint32_t)kMaxPairs;
-  uint32_t i = 0;
-  int kind = NEAR_DONE;
-  NearPair np = {};
+// P3b driver: pairs in order; a mesh pair's leaves one by one, each leaf's contact added in order.  The loop is kept
+// as a state (P3bLoop) and a step (one leaf of the current mesh job, or the next pairs up to one that opens a job), so
+// that a kernel can step the loops of many arenas in lockstep; phase3b runs the steps to the end.
+struct P3bLoop {
+  uint32_t n, i, unimplemented;
+  int kind;
+  NearPair np;
   BoxJob bj;
   SphereJob sj;
-  while (kind != NEAR_DONE || i < n) {
-    if (kind == NEAR_DONE) {
-      RSX_ZONE_BEGIN(z_head);
-      while (i < n) {
-        Pair p = S.pairs[i++];
-        kind = near_head(c, D.proxies[p.h0].body, D.proxies[p.h1].body, np, bj, sj);
-        if (kind != NEAR_DONE) break;
-      }
-      RSX_ZONE_END(z_head, 10);
-      if (kind == NEAR_DONE) break;
+};
+RSX_F void p3b_begin(const ArenaState& S, P3bLoop& L) {
+  L.n = S.n_pairs < (uint32_t)kMaxPairs ? S.n_pairs : (uint32_t)kMaxPairs;
+  L.i = 0;
+  L.unimplemented = 0;
+  L.kind = NEAR_DONE;
+  L.np = NearPair{};
+}
+// one step; false when the phase has no work left
+RSX_F bool p3b_step(ArenaState& S, const StaticData& D, P3bLoop& L) {
+  if (!(L.kind != NEAR_DONE || L.i < L.n)) return false;
+  Ctx c = {S, D, L.unimplemented};
+  NearPair& np = L.np;
+  BoxJob& bj = L.bj;
+  SphereJob& sj = L.sj;
+  if (L.kind == NEAR_DONE) {
+    RSX_ZONE_BEGIN(z_head);
+    while (L.i < L.n) {
+      Pair p = S.pairs[L.i++];
+      L.kind = near_head(c, D.proxies[p.h0].body, D.proxies[p.h1].body, np, bj, sj);
+      if (L.kind != NEAR_DONE) break;
     }
-    uint32_t tri;
-    if (kind == NEAR_BOX_JOB) {
-      RSX_ZONE_BEGIN(z_bnext);
-      bool more = box_job_next(D, bj, &tri);
-      RSX_ZONE_END(z_bnext, 12);
-      if (more) {
-        RSX_ZONE_BEGIN(z_sat);
-        const Tri& t = D.tris[bj.mesh->tri_first + tri];
-        V3 q[3] = {xform_point(bj.mesh_to_box, t.p0), xform_point(bj.mesh_to_box, t.p1), xform_point(bj.mesh_to_box, t.p2)};
-        SatHit h;
-        if (box_triangle_sat(bj.box_xf, bj.half, bj.margin, q, bj.maxd, &h)) {
-          if (!bj.has_m) {
-            bj.m = manifold_new(bj.car, bj.mesh_body);
-            bj.has_m = true;
-          }
-          add_contact(c, bj.m, bj.car, bj.mesh_body, bj.tri_rot * t.n, h.point_world, h.distance, (int32_t)tri);
-        }
-        RSX_ZONE_END(z_sat, 11);
-      } else {
-        RSX_ZONE_BEGIN(z_btail);
-        Manifold fresh = {};
-        bool has = false;
-        if (bj.has_m) {
-          refresh_points(S, D, bj.m, bj.car, bj.mesh_body);
-          if (bj.m.n != 0) {
-            fresh = bj.m;
-            has = true;
-          }
-        }
-        near_tail(c, np.rb0, np.rb1, np.cached, has, fresh);
-        kind = NEAR_DONE;
-        RSX_ZONE_END(z_btail, 13);
-      }
-    } else {
-      RSX_ZONE_BEGIN(z_snext);
-      bool more = cursor_next(sj.cu, D, *sj.mesh, sj.box, &tri);
-      RSX_ZONE_END(z_snext, 14);
-      if (more) {
-        RSX_ZONE_BEGIN(z_stri);
-        SphereTriHit h;
-        if (sphere_triangle(D.tris[sj.mesh->tri_first + tri], sj.center, sj.radius, sj.rt, sj.rt2, &h))
-          add_contact(c, S.manifolds[sj.manifold], sj.sph, sj.mesh_body, h.normal, h.point + sj.mesh_t, h.depth, (int32_t)tri);
-        RSX_ZONE_END(z_stri, 15);
-      } else {
-        RSX_ZONE_BEGIN(z_stail);
-        Manifold& m = S.manifolds[sj.manifold];
-        if (m.n != 0) refresh_points(S, D, m, sj.sph, sj.mesh_body);
-        push_active(S, (uint32_t)sj.manifold);
-        kind = NEAR_DONE;
-        RSX_ZONE_END(z_stail, 16);
-      }
+    RSX_ZONE_END(z_head, 10);
+    if (L.kind == NEAR_DONE) {
+      L.unimplemented = c.unimplemented;
+      return false;
     }
   }
-  return c.unimplemented;
+  uint32_t tri;
+  if (L.kind == NEAR_BOX_JOB) {
+    RSX_ZONE_BEGIN(z_bnext);
+    bool more = box_job_next(D, bj, &tri);
+    RSX_ZONE_END(z_bnext, 12);
+    if (more) {
+      RSX_ZONE_BEGIN(z_sat);
+      const Tri& t = D.tris[bj.mesh->tri_first + tri];
+      V3 q[3] = {xform_point(bj.mesh_to_box, t.p0), xform_point(bj.mesh_to_box, t.p1), xform_point(bj.mesh_to_box, t.p2)};
+      SatHit h;
+      if (box_triangle_sat(bj.box_xf, bj.half, bj.margin, q, bj.maxd, &h)) {
+        if (!bj.has_m) {
+          bj.m = manifold_new(bj.car, bj.mesh_body);
+          bj.has_m = true;
+        }
+        add_contact(c, bj.m, bj.car, bj.mesh_body, bj.tri_rot * t.n, h.point_world, h.distance, (int32_t)tri);
+      }
+      RSX_ZONE_END(z_sat, 11);
+    } else {
+      RSX_ZONE_BEGIN(z_btail);
+      Manifold fresh = {};
+      bool has = false;
+      if (bj.has_m) {
+        refresh_points(S, D, bj.m, bj.car, bj.mesh_body);
+        if (bj.m.n != 0) {
+          fresh = bj.m;
+          has = true;
+        }
+      }
+      near_tail(c, np.rb0, np.rb1, np.cached, has, fresh);
+      L.kind = NEAR_DONE;
+      RSX_ZONE_END(z_btail, 13);
+    }
+  } else {
+    RSX_ZONE_BEGIN(z_snext);
+    bool more = cursor_next(sj.cu, D, *sj.mesh, sj.box, &tri);
+    RSX_ZONE_END(z_snext, 14);
+    if (more) {
+      RSX_ZONE_BEGIN(z_stri);
+      SphereTriHit h;
+      if (sphere_triangle(D.tris[sj.mesh->tri_first + tri], sj.center, sj.radius, sj.rt, sj.rt2, &h))
+        add_contact(c, S.manifolds[sj.manifold], sj.sph, sj.mesh_body, h.normal, h.point + sj.mesh_t, h.depth, (int32_t)tri);
+      RSX_ZONE_END(z_stri, 15);
+    } else {
+      RSX_ZONE_BEGIN(z_stail);
+      Manifold& m = S.manifolds[sj.manifold];
+      if (m.n != 0) refresh_points(S, D, m, sj.sph, sj.mesh_body);
+      push_active(S, (uint32_t)sj.manifold);
+      L.kind = NEAR_DONE;
+      RSX_ZONE_END(z_stail, 16);
+    }
+  }
+  L.unimplemented = c.unimplemented;
+  return L.kind != NEAR_DONE || L.i < L.n;
+}
+
+RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {
+  P3bLoop L;
+  p3b_begin(S, L);
+  while (p3b_step(S, D, L)) {
+  }
+  return L.unimplemented;
 }
 
 }  // namespace sim
