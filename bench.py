@@ -34,6 +34,7 @@ ARENAS = 65536
 TICK_BYTES = 2567 * 4
 ALG_BYTES_PER_ARENA_TICK = (TICK_BYTES * 2 + 64 + 4) / 8.0  # state in + out, controls, result, per tick
 METRIC = "arena-ticks/s, 8-tick decision, 65,536 arenas: binned vs plain, bit-exact"
+TRAFFIC_PER_ARENA_DECISION = 4.585e9 / 32768
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
 
@@ -258,8 +259,12 @@ def run_ours(args):
     tune_ctl = [torch.from_numpy(rsx.decision_controls(args.seed * 1000 + 700 + rank, d, n).view(np.int32)).to(dev.device) for d in range(2)]
     torch.cuda.synchronize()
     if args.mode in ("binned", "lockstep") and not args.no_tune:
+        # tuned on the states the timed decisions start from (after the warm-up decisions), with controls of their own
+        run.restore(start)
+        for s_ in range(args.warmup):
+            run.step(dctl[s_].data_ptr(), {"mode": "plain", "block": args.plain_block})
         cands = run.candidates(binning=args.mode == "binned")
-        tuned = run.tune([c.data_ptr() for c in tune_ctl], cands)
+        tuned = run.tune([c.data_ptr() for c in tune_ctl], cands, repeats=2)
         config = dict(run.config)
         tune_top = [{"ms": round(ms, 3), **c} for ms, c in tuned[:6]]
     elif args.mode == "plain":
@@ -347,7 +352,11 @@ def run_ours(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 2), from the ncu capture in
+    # profiles/k_sim8_lockstep_headline.md: 4.585 GB for 32,768 arenas, scaled by the arena count
+    traffic = TRAFFIC_PER_ARENA_DECISION * n if config["mode"] != "plain" else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled from 32,768 arenas)",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": mean_ms}
 
