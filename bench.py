@@ -173,6 +173,7 @@ def run_ours(args):
     import torch
     import rsx
     import predictor as P
+    import replicas
     from runner import DecisionRunner
 
     rank = int(os.environ.get("RANK", "0"))
@@ -203,11 +204,7 @@ def run_ours(args):
             dist.barrier()
 
     def reduce_max(x):
-        if not dist:
-            return x
-        tt = torch.tensor([x], device=dev.device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return replicas.max_over_ranks(x, dist, dev.device)
 
     def timed(config, graph=False, clk=None):
         """W warm-up + K timed decisions of `config` from the start states; (device ms of the K, per-step ms)."""
@@ -273,10 +270,7 @@ def run_ours(args):
     else:
         config = {"mode": args.mode, "block": args.block, "grid": args.grid or run.sms, "split": args.split, "threshold": args.threshold}
         tune_top = None
-    if dist:  # every rank runs rank 0's configuration
-        obj = [config]
-        dist.broadcast_object_list(obj, src=0)
-        config = obj[0]
+    config = replicas.broadcast_config(config, dist, dev.device)  # every rank runs rank 0's configuration
 
     # ---- timing: the plain launch, the best unbinned lockstep, then the chosen configuration ----
     modes = {}
