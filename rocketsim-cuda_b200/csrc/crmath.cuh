@@ -11,6 +11,8 @@
 //   * Payne-Hanek reduction of x by pi/2 against 384 bits of 2/pi;
 //   * sin / cos: a 1/64-spaced table of sin and cos, and Taylor series of the remainder (|d| <= 1/128);
 //   * tan: sin / cos by restoring long division of the two fixed-point values;
+//   * fast paths for sin / cos / tan (|x| in [2^-14, 64]) and atan2 (normal operands): double-float evaluation with a
+//     proven error bound and a rounding test; only when the test cannot decide does the fixed-point path run;
 //   * atan: a 1/128-spaced table of atan and atan((t - c) / (1 + t c)) by its Taylor series;
 //   * pow: 2^(y log2 x): log2 by a table of log2(1 + i/128) and the ln(1 + v) series; exp2 by a table of 2^(j/128)
 //     and the exp series; exact results (pow has them) are detected as ties within 2^-100.
@@ -315,7 +317,9 @@ RSX_F bool rounds_to(DF v, float err, float* out) {
 RSX_F float round_nearest(float v) {  // v < 2^22: the nearest integer, ties away (only the quadrant's parity matters)
   return i2f(f2i(fadd(v, 0.5f)));
 }
-RSX_F bool sincos_fast(float ax, bool want_s, bool want_c, float* s_out, float* c_out) {
+// sin and cos of ax in [2^-14, 64] as float pairs, and the absolute error the reduction adds (each value's own error
+// is below |value| * 1e-12 besides)
+RSX_F void sincos_df(float ax, DF* s_out, DF* c_out, float* red_err_out) {
   float rh = ax, rl = 0.0f, red_err = 0.0f;
   int q = 0;
   if (ax > 0.78539816f) {
@@ -353,15 +357,69 @@ RSX_F bool sincos_fast(float ax, bool want_s, bool want_c, float* s_out, float* 
   S = quick_sum(S.h, fadd(S.l, fadd(cx.l, fmul(rl, C.h))));
   C = quick_sum(C.h, fsub(C.l, fmul(rl, fadd(rh, cx.h))));
   // quadrant
-  DF vs = (q == 0) ? S : (q == 1) ? C : (q == 2) ? DF{fneg(S.h), fneg(S.l)} : DF{fneg(C.h), fneg(C.l)};
-  DF vc = (q == 0) ? C : (q == 1) ? DF{fneg(S.h), fneg(S.l)} : (q == 2) ? DF{fneg(C.h), fneg(C.l)} : S;
+  *s_out = (q == 0) ? S : (q == 1) ? C : (q == 2) ? DF{fneg(S.h), fneg(S.l)} : DF{fneg(C.h), fneg(C.l)};
+  *c_out = (q == 0) ? C : (q == 1) ? DF{fneg(S.h), fneg(S.l)} : (q == 2) ? DF{fneg(C.h), fneg(C.l)} : S;
+  *red_err_out = red_err;
+}
+RSX_F bool sincos_fast(float ax, bool want_s, bool want_c, float* s_out, float* c_out) {
+  DF vs, vc;
+  float red_err;
+  sincos_df(ax, &vs, &vc, &red_err);
   bool ok = true;
   if (want_s) ok = ok && rounds_to(vs, fadd(fmul(fabs_(vs.h), 1e-12f), red_err), s_out);
   if (want_c) ok = ok && rounds_to(vc, fadd(fmul(fabs_(vc.h), 1e-12f), red_err), c_out);
   return ok;
 }
 
+// a / b in float pairs (Dekker's division: the quotient of the leading parts, corrected by the remainder's quotient);
+// relative error below 2^-44 for normal operands
+RSX_F DF df_div(DF a, DF b) {
+  float q1 = fdiv(a.h, b.h);
+  DF p = df_mul_f(b, q1);
+  DF r = df_add(a, DF{fneg(p.h), fneg(p.l)});
+  float q2 = fdiv(r.h, b.h);
+  return quick_sum(q1, q2);
+}
+
+// tan of ax in [2^-14, 64] as sin / cos in float pairs; false when the error bound does not decide the rounding (near
+// a pole the cosine's relative error grows and the test fails)
+RSX_F bool tan_fast(float ax, float* out) {
+  DF vs, vc;
+  float red_err;
+  sincos_df(ax, &vs, &vc, &red_err);
+  float as = fabs_(vs.h), ac = fabs_(vc.h);
+  if (ac < 1e-6f || as < 1e-30f) return false;
+  DF t = df_div(vs, vc);
+  float rel = fadd(fadd(fdiv(fadd(fmul(as, 1e-12f), red_err), as), fdiv(fadd(fmul(ac, 1e-12f), red_err), ac)), 1e-12f);
+  return rounds_to(t, fmul(fabs_(t.h), rel), out);
+}
+
 // ---- atan2 ---------------------------------------------------------------------------------------------------------
+
+// fast path of atan2 for |y|, |x| in [2^-63, 2^64) with exponents at most 60 apart: t = min / max (float pair, the
+// remainder of the rounded quotient is exact), c = the nearest multiple of 1/128, atan t = atan c + atan u with
+// u = (t - c) / (1 + t c), |u| <= 1/256, atan u = u - u^3/3 + u^5/5 - u^7/7; then pi/2 - . when |y| > |x| and pi - .
+// when x < 0.  The error is below 2^-38 of the result; the rounding test uses 2^-36.  The magnitude goes to *out.
+RSX_F bool atan2_fast(uint32_t ay, uint32_t ax, bool xneg, float* out) {
+  int ey = (int)(ay >> 23), ex = (int)(ax >> 23);
+  // operands in [2^-63, 2^64): the quotient's remainder and every product below stay normal (exact where it matters)
+  if (ey < 64 || ex < 64 || ey > 190 || ex > 190 || ey - ex > 60 || ex - ey > 60) return false;
+  bool swap = ay > ax;
+  float num = from_bits(swap ? ax : ay), den = from_bits(swap ? ay : ax);
+  float th = fdiv(num, den);
+  float tl = fdiv(ffma(fneg(th), den, num), den);
+  int i = (int)f2i(fadd(fmul(th, 128.0f), 0.5f));
+  float c = fmul(i2f(i), 0.0078125f);
+  DF tc = two_prod(th, c);
+  tc = quick_sum(tc.h, fadd(tc.l, fmul(tl, c)));
+  DF u = df_div(two_sum(fsub(th, c), tl), df_add(DF{1.0f, 0.0f}, tc));
+  float p = fmul(u.h, u.h);
+  float sfac = fmul(p, fadd(-0.33333334f, fmul(p, fadd(0.2f, fmul(p, -0.14285715f)))));
+  DF r = df_add(df_c(kAtan128DF[i]), quick_sum(u.h, fadd(u.l, fmul(u.h, sfac))));
+  if (swap) r = df_add(df_c(kPiDF[0]), DF{fneg(r.h), fneg(r.l)});
+  if (xneg) r = df_add(df_c(kPiDF[1]), DF{fneg(r.h), fneg(r.l)});
+  return rounds_to(r, fmul(fabs_(r.h), 1.5e-11f), out);
+}
 
 // atan(t) for t = m * 2^te with m in [1, 2) (fixed point) and t <= 1, as an absolute fixed-point value; for tiny t the
 // value is returned relative: *rel = true and the result is m' * 2^(*re) with m' in fixed point.
@@ -462,6 +520,8 @@ RSX_F float atan2f_cr(float y, float x) {
     return from_bits(PI2_B | sy);
   }
   if (ax == 0x7F800000u) return from_bits((xneg ? PI_B : 0u) | sy);
+  float fast;
+  if (atan2_fast(ay, ax, xneg, &fast)) return from_bits(bits(fast) | sy);
   int e, dir;
   U128 v = atan2_mag(ay, ax, xneg, &e, &dir);
   return from_bits(round_f32(v, e, dir, 0, 0) | sy);
@@ -603,6 +663,10 @@ RSX_HD RSX_NOINL inline float atan2_via_double(float a0, float a1) {
   bool xneg = (bx >> 31) != 0;
   if (ay > 0x7F800000u || ax > 0x7F800000u || ay == 0 || ax == 0 || ay == 0x7F800000u || ax == 0x7F800000u)
     return atan2f_cr(a0, a1);  // the special values are exact doubles whose float rounding is atan2f's
+  // the fast path's rounding test keeps a margin of 1e-4 half-gaps, far above the 2^-53 the double rounding can move
+  // the value, so its float is also the float of the rounded double
+  float fast;
+  if (atan2_fast(ay, ax, xneg, &fast)) return from_bits(bits(fast) | sy);
   int e, dir;
   U128 v = atan2_mag(ay, ax, xneg, &e, &dir);
   return from_bits(round_f32(v, e, dir, 53, 0) | sy);
@@ -617,6 +681,19 @@ RSX_HD RSX_NOINL inline float hypot_via_double(float a, float b) {
   }
   if (ua < ub) { uint32_t t = ua; ua = ub; ub = t; }
   if (ua == 0) return 0.0f;
+  if ((ua >> 23) <= 187 && (ub >> 23) >= 91) {
+    // fast path, both in [2^-36, 2^61) (the products' low parts stay normal, so they are exact): a^2 + b^2 from exact
+    // products as a float pair, its square root corrected by one
+    // Newton step (relative error below 2^-44); the rounding test's margin covers the double rounding as above
+    float fa = from_bits(ua), fb = from_bits(ub);
+    DF s2 = df_add(two_prod(fa, fa), two_prod(fb, fb));
+    float r0 = fsqrt(s2.h);
+    DF rr = two_prod(r0, r0);
+    float d = fadd(fsub(fsub(s2.h, rr.h), rr.l), s2.l);
+    DF h = quick_sum(r0, fdiv(d, fmul(2.0f, r0)));
+    float fast;
+    if (rounds_to(h, fmul(h.h, 1.5e-11f), &fast)) return fast;
+  }
   auto unpack = [](uint32_t v, uint64_t* m, int* e) {  // v = m * 2^e, m integer
     int be = (int)(v >> 23);
     uint32_t mm = v & 0x7FFFFFu;
@@ -690,7 +767,14 @@ RSX_HD RSX_NOINL inline float cr_cos(float x) {
   if (ax >= 0x38800000u && ax <= 0x42800000u && crm::sincos_fast(from_bits(ax), false, true, &ss, &cc)) return cc;
   return crm::trig(x, 1);
 }
-RSX_HD RSX_NOINL inline float cr_tan(float x) { return crm::trig(x, 2); }
+RSX_HD RSX_NOINL inline float cr_tan(float x) {
+  uint32_t ax = bits(x) & 0x7FFFFFFFu;
+  if (ax >= 0x38800000u && ax <= 0x42800000u) {  // 2^-14 <= |x| <= 64
+    float t;
+    if (crm::tan_fast(from_bits(ax), &t)) return from_bits(bits(t) ^ (bits(x) & 0x80000000u));
+  }
+  return crm::trig(x, 2);
+}
 RSX_HD RSX_NOINL inline float cr_atan2(float y, float x) { return crm::atan2f_cr(y, x); }
 RSX_HD RSX_NOINL inline float cr_pow(float x, float y) { return crm::powf_cr(x, y); }
 

@@ -24,6 +24,8 @@ def probe():
     for f in ("rsref_atan2f", "rsref_powf", "rsref_atan2_64_f", "rsref_hypot64_f"):
         getattr(L, f).restype = ctypes.c_float
         getattr(L, f).argtypes = [ctypes.c_float, ctypes.c_float]
+    for f in ("rsref_atan2f_batch", "rsref_atan2_64_f_batch", "rsref_hypot64_f_batch"):
+        getattr(L, f).argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong]
     return L
 
 
@@ -70,6 +72,46 @@ def test_binary_matches_reference(rsx, probe, fn, name):
     got = mine(rsx, fn, a, b)
     bad = ~same(want, got)
     assert not bad.any(), f"{bad.sum()} mismatches, first a={a[bad][:3]} b={b[bad][:3]}"
+
+
+@pytest.mark.parametrize("fn,name", [(3, "rsref_atan2f_batch"), (5, "rsref_atan2_64_f_batch"), (6, "rsref_hypot64_f_batch")])
+def test_fast_path_domains(rsx, probe, fn, name):
+    """2M pairs in the double-float fast paths' domains (atan2: operands in [2^-63, 2^64), exponents at most 60 apart;
+    hypot: [2^-36, 2^61)): near the diagonal, near the axes, all quadrants, and the game's magnitudes; atan2f, the
+    auto-flip's float(double atan2) and float(double hypot), bit for bit against the reference."""
+    rng = np.random.default_rng(77)
+    n = 400000
+    sign = lambda k: np.where(rng.integers(0, 2, k) == 1, np.uint32(0x80000000), np.uint32(0))
+    mant = lambda k: rng.integers(0, 1 << 23, k).astype(np.uint32)
+    parts_y, parts_x = [], []
+    e1 = rng.integers(107, 148, n)
+    parts_y.append(e1)
+    parts_x.append(rng.integers(107, 148, n))
+    e2 = rng.integers(120, 130, n)  # near the diagonal
+    parts_y.append(e2)
+    parts_x.append(e2)
+    e3 = rng.integers(127, 137, n)  # near the axes
+    parts_y.append(e3)
+    parts_x.append(e3 - rng.integers(0, 61, n))
+    e4 = rng.integers(64, 191, n)
+    parts_y.append(e4)
+    parts_x.append(np.clip(e4 + rng.integers(-60, 61, n), 64, 190))
+    ey = np.concatenate(parts_y).astype(np.uint32)
+    ex = np.concatenate(parts_x).astype(np.uint32)
+    m = ey.size
+    my = mant(m)
+    mx = mant(m)
+    near = slice(n, 2 * n)
+    mx[near] = (my[near] + rng.integers(-32, 33, n).astype(np.uint32)) & np.uint32(0x7FFFFF)
+    y = (sign(m) | (ey << np.uint32(23)) | my).view(np.float32)
+    x = (sign(m) | (ex << np.uint32(23)) | mx).view(np.float32)
+    y = np.concatenate([y, rng.uniform(-3000, 3000, n).astype(np.float32)])
+    x = np.concatenate([x, rng.uniform(-3000, 3000, n).astype(np.float32)])
+    want = np.zeros_like(y)
+    getattr(probe, name)(y.ctypes.data, x.ctypes.data, want.ctypes.data, y.size)
+    got = mine(rsx, fn, y, x)
+    bad = ~same(want, got)
+    assert not bad.any(), f"{bad.sum()} mismatches, first y={y[bad][:3]} x={x[bad][:3]}"
 
 
 def test_damping_factor_exact(rsx, probe):
