@@ -415,7 +415,6 @@ RSX_F int pad_winner(const ArenaState& S, int p, float mx) {
 RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
   const float mx = D.mut[M_MAX_BOOST];
   int touching[kCars] = {-1, -1};
-  int winner[kPads];
   for (int i = 0; i < kPads; ++i) {
     const PadConst& pad = D.pads[i];
     PadTouch& t = S.pad_touch[i];
@@ -429,8 +428,10 @@ RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
         t.car[kept++] = ci;
       }
     }
-    for (uint32_t k = kept; k < t.n; ++k) t.car[k] = 0;
-    t.n = kept;
+    if (kept != t.n) {  // (an unchanged list is left as it is: the same words, no stores)
+      for (uint32_t k = kept; k < t.n; ++k) t.car[k] = 0;
+      t.n = kept;
+    }
   }
   for (int ci = 0; ci < kCars; ++ci) {
     const Car& car = S.cars[ci];
@@ -450,12 +451,14 @@ RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
       break;
     }
   }
-  for (int i = 0; i < kPads; ++i) winner[i] = pad_winner(S, i, mx);
+  // Each pad's winner is the first car of its list that can take boost.  A car is listed at one pad at most (its
+  // `touching` pad), so a pickup changes only that pad's winner: evaluating the winner of a car's own pad when the car
+  // is reached gives what a table made before the loop and refreshed after each pickup would hold.
   for (int ci = 0; ci < kCars; ++ci) {
     Car& car = S.cars[ci];
     if (car.is_demoed || car.boost >= mx) continue;
     int i = touching[ci];
-    if (i < 0 || winner[i] != ci) continue;
+    if (i < 0 || pad_winner(S, i, mx) != ci) continue;
     const PadConst& pad = D.pads[i];
     int64_t tick = (int64_t)u64_of(S.tick_count);
     if (S.pad_gave[i].some) {
@@ -466,7 +469,6 @@ RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
     S.pad_gave[i].some = 1;
     S.pad_gave[i].v = u64w((uint64_t)tick);
     S.events |= 1u << (EV_PICKUP + ci);
-    winner[i] = pad_winner(S, i, mx);
   }
 }
 

@@ -436,10 +436,11 @@ RSX_F Box3 proxy_box(const ArenaState& S, const StaticData& D, uint32_t h) {
     if (D.dyn_handle[d] == h) return S.dyn_proxy[d].box;
   return D.proxies[h].box;
 }
-RSX_F void ray_candidate(const ArenaState& S, const StaticData& D, uint32_t h, RayPacket* pk) {
+// the ray test's filter of a candidate handle: not the ignored body, and group / mask agree both ways
+RSX_F bool ray_accepts(const StaticData& D, uint32_t h, const RayPacket* pk) {
   const ProxyConst& px = D.proxies[h];
-  if (pk->ignore == px.body) return;
-  if ((px.group & pk->mask) != 0 && (pk->group & px.mask) != 0) ray_body(S, D, px.body, pk);
+  if (pk->ignore == px.body) return false;
+  return (px.group & pk->mask) != 0 && (pk->group & px.mask) != 0;
 }
 
 // the grid's candidate walk: one cell per distinct ray source, its static handles, then its dynamic ones
@@ -461,7 +462,10 @@ RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
     for (int k = 0; k < nc; ++k) seen = seen || cells[k] == c;
     if (!seen) cells[nc++] = c;
   }
-  uint32_t seen = 0;
+  // the candidates in walk order first (nothing in the walk depends on the hits), then one body test per step, so that
+  // the lanes of a warp step through their lists together
+  uint32_t seen = 0, cand[kHandles];
+  int nk = 0;
   for (int ci = 0; ci < nc; ++ci) {
     uint32_t cell = cells[ci];
     const CellRange& cr = D.cells[cell];
@@ -469,16 +473,17 @@ RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
       uint32_t h = D.cell_handles[cr.first + e];
       if (seen & (1u << h)) continue;
       seen |= 1u << h;
-      if (box_overlap(rbx, proxy_box(S, D, h))) ray_candidate(S, D, h, pk);
+      if (box_overlap(rbx, proxy_box(S, D, h)) && ray_accepts(D, h, pk)) cand[nk++] = D.proxies[h].body;
     }
     for (uint32_t e = 0; e < S.n_dyn_cells; ++e) {
       if (S.dyn_cells[e].cell != cell) continue;
       uint32_t h = S.dyn_cells[e].handle;
       if (seen & (1u << h)) continue;
       seen |= 1u << h;
-      if (box_overlap(rbx, proxy_box(S, D, h))) ray_candidate(S, D, h, pk);
+      if (box_overlap(rbx, proxy_box(S, D, h)) && ray_accepts(D, h, pk)) cand[nk++] = D.proxies[h].body;
     }
   }
+  for (int k = 0; k < nk; ++k) ray_body(S, D, cand[k], pk);
 }
 
 struct WheelHit {
