@@ -133,6 +133,13 @@ int rsx_sim8_persistent_noalloc(uint32_t* d_states, uint32_t n, const void* d_st
 int rsx_profile_phases_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                            const rsx_controls* d_controls, uint64_t* d_phase_cycles, void* stream);
 
+/* Device resets (no counterpart in the reference): the arenas selected by d_mask (u8, nonzero: reset; null: all) and
+ * by d_result (the last decision's result words; null: no condition, else only arenas whose decision scored) get the
+ * start state rsx_make_states_multi builds for the same seed, arena index, StaticData and mix[5] (host memory),
+ * written into the AoSoA-32 buffer (all 2784 words); d_reset_count (nullable) is incremented per reset arena. */
+int rsx_reset_arenas_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, uint64_t seed,
+                         const float* mix, const uint32_t* d_result, const uint8_t* d_mask, uint32_t* d_reset_count, void* stream);
+
 /* ---- the contact predictor (no counterpart in the reference: the binning it drives is this library's) ----
  * A 48 -> 128 -> 128 -> 128 -> 6 ReLU MLP (sigmoid outputs) over per-arena features, BF16 weights and activations
  * with FP32 accumulation, trained on the decision kernels' event-OR labels.  Weights: RSX_PRED_PARAMS FP32 master

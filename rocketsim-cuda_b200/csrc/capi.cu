@@ -40,6 +40,8 @@ cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const f
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t* block_scratch, uint32_t* order, uint32_t* heavy_total,
                                 cudaStream_t s);
+cudaError_t rsx_launch_reset_arenas(uint32_t* states, uint32_t n, const void* sds, const uint8_t* sd_index, uint64_t seed, const float* mix,
+                                    const uint32_t* result, const uint8_t* mask, uint32_t* reset_count, cudaStream_t s);
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
 cudaError_t rsx_launch_phase(int k, uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
 cudaError_t rsx_launch_step_tick(uint32_t* buf, const void* sd, uint32_t n, int32_t* status, cudaStream_t s);
@@ -286,6 +288,14 @@ int rsx_copy_raw(void* d_dst, const void* d_src, uint64_t bytes, void* stream) {
   if (!d_dst || !d_src) return RSX_E_ARG;
   if (bytes == 0) return RSX_OK;
   RSX_CK(cudaMemcpyAsync(d_dst, d_src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_reset_arenas_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, uint64_t seed, const float* mix,
+                         const uint32_t* d_result, const uint8_t* d_mask, uint32_t* d_reset_count, void* stream) {
+  if (!d_states || !d_statics || !mix) return RSX_E_ARG;
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_reset_arenas(d_states, n, d_statics, d_sd_index, seed, mix, d_result, d_mask, d_reset_count, (cudaStream_t)stream));
   return RSX_OK;
 }
 

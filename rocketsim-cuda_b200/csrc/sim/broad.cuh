@@ -281,7 +281,7 @@ RSX_F void set_body_pose(Body& b, const BodyConst& c, const Aff& xf, V3 lin_vel,
   b.damp_cache_value = 0.0f;
 }
 
-inline void init_broadphase(ArenaState& S, const StaticData& D) {
+RSX_HD inline void init_broadphase(ArenaState& S, const StaticData& D) {
   Box3 boxes[kHandles];
   for (int h = 1; h < kHandles; ++h) boxes[h] = D.proxies[h].box;
   const V3 cbt = vs(kBreakingThreshold);
