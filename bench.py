@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=2, help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step")
+    ap.add_argument("--split", type=int, default=6,
+                    help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain launch's comparison timing")
     ap.add_argument("--cpu-sample", type=int, default=0, help="reference arm: arenas per step (0: all)")

@@ -7,7 +7,9 @@
 // active 4% of cycles).  Here the warps of a block step their arenas phase by phase together: a __syncthreads()
 // after each of the ten phases (split 1: also after each car's pre-tick inside P1; split 2: P1 of each car in three
 // parts, pre-tick head / wheel rays / wheel response; split 3: also a barrier after every step of P3b's pair / leaf
-// loop), so that at any time the block's warps fetch from one piece of code.
+// loop; split 6: split 2 with P5 as rows / iterations / integration and P8 as cars / the rest; splits 4 and 5 leave
+// the barriers out between P3b (4) or P4 (5) and P8, to measure what they buy), so that at any time the block's warps
+// fetch from one piece of code.
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -100,6 +102,31 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
       }
 #pragma unroll 1
       for (int k = 2; k < sim::kPhases; ++k) {
+        // split 4: no barrier between P3b and P8 (warps without contact work run ahead to the tick's end);
+        // split 5: none between P4 and P8
+        const bool bar = !((SPLIT == 4 && k >= 4 && k < sim::kPhases - 1) || (SPLIT == 5 && k >= 5 && k < sim::kPhases - 1));
+        if (SPLIT == 6 && k == 6) {  // P5: rows, iterations, integration
+          sim::Solver sv;
+          if (have) sim::t_p5_setup(s, *D, sv);
+          __syncthreads();
+          if (have) sim::t_p5_iterate(sv);
+          __syncthreads();
+          if (have) sim::t_p5_finish(s, *D, sv);
+          __syncthreads();
+          continue;
+        }
+        if (SPLIT == 6 && k == 9) {  // P8: cars, then pads / ball / tick count
+          if (have) sim::t_p8_cars(s);
+          __syncthreads();
+          if (have) sim::t_p8_rest(s, *D);
+          __syncthreads();
+          continue;
+        }
+        if (SPLIT == 4 || SPLIT == 5) {
+          if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
+          if (bar) __syncthreads();
+          continue;
+        }
         if (SPLIT == 3 && k == 4) {
           // P3b with a barrier after every step of the pair / leaf loop
           sim::P3bLoop L;
@@ -172,7 +199,13 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
                    const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split == 3)
+  if (split == 6)
+    K_NAME<6><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 5)
+    K_NAME<5><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 4)
+    K_NAME<4><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 3)
     K_NAME<3><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
   else if (split == 2)
     K_NAME<2><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);

@@ -472,11 +472,14 @@ RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
   }
 }
 
-RSX_F void phase8(ArenaState& S, const StaticData& D) {
+// P8 in two steps a kernel can barrier between (the cars, then pads, ball and tick count); phase8 runs both.
+RSX_F void phase8_cars(ArenaState& S) {
   for (int ci = 0; ci < kCars; ++ci) {
     car_post_tick(S.cars[ci], S.bodies[1 + ci]);
     car_finish(S.cars[ci], S.bodies[1 + ci]);
   }
+}
+RSX_F void phase8_rest(ArenaState& S, const StaticData& D) {
   if (D.pads_enabled) pads_tick(S, D);
   const Body& rb = S.bodies[0];
   S.ball.vel = rb.lin_vel * kBTtoUU;
@@ -485,6 +488,10 @@ RSX_F void phase8(ArenaState& S, const StaticData& D) {
   S.ball.rot = rb.xf.m;
   S.ball.ticks_since_kickoff = u64w(u64_of(S.ball.ticks_since_kickoff) + 1);
   S.tick_count = u64w(u64_of(S.tick_count) + 1);
+}
+RSX_F void phase8(ArenaState& S, const StaticData& D) {
+  phase8_cars(S);
+  phase8_rest(S, D);
 }
 
 }  // namespace sim

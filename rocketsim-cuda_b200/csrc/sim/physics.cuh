@@ -22,6 +22,11 @@ RSX_HD RSX_NOINL inline uint32_t t_p3b(ArenaState& S, const StaticData& D) { ret
 RSX_HD RSX_NOINL inline bool t_p3b_step(ArenaState& S, const StaticData& D, P3bLoop& L) { return p3b_step(S, D, L); }
 RSX_HD RSX_NOINL inline void t_p4(ArenaState& S, const StaticData& D) { phase4(S, D); }
 RSX_HD RSX_NOINL inline void t_p5(ArenaState& S, const StaticData& D) { phase5(S, D); }
+RSX_HD RSX_NOINL inline void t_p5_setup(ArenaState& S, const StaticData& D, Solver& sv) { phase5_setup(S, D, sv); }
+RSX_HD RSX_NOINL inline void t_p5_iterate(Solver& sv) { phase5_iterate(sv); }
+RSX_HD RSX_NOINL inline void t_p5_finish(ArenaState& S, const StaticData& D, Solver& sv) { phase5_finish(S, D, sv); }
+RSX_HD RSX_NOINL inline void t_p8_cars(ArenaState& S) { phase8_cars(S); }
+RSX_HD RSX_NOINL inline void t_p8_rest(ArenaState& S, const StaticData& D) { phase8_rest(S, D); }
 RSX_HD RSX_NOINL inline void t_p6(ArenaState& S, const StaticData& D) { phase6(S, D); }
 RSX_HD RSX_NOINL inline void t_p7(ArenaState& S, const StaticData& D) { phase7(S, D); }
 RSX_HD RSX_NOINL inline void t_p8(ArenaState& S, const StaticData& D) { phase8(S, D); }

@@ -380,9 +380,10 @@ RSX_F void emit_special(Solver& sv, ArenaState& S, const StaticData& D, const Sp
   sv.fric[sv.nf++] = friction_row(ia, ib, sa, sb, s0, s1, r1, r2, cp.friction, lat, fi);
 }
 
-RSX_F void phase5(ArenaState& S, const StaticData& D) {
+// P5 in three steps a kernel can barrier between: the rows (setup), the split-impulse and PGS iterations, and the
+// integration of the results (finish); phase5 runs them in order.
+RSX_F void phase5_setup(ArenaState& S, const StaticData& D, Solver& sv) {
   const float dt = fdiv(1.0f, 120.0f);
-  Solver sv;
   sv.nb = sv.nc = sv.nf = sv.ns = 0;
   sv.fixed = kNone;
   // bodies: the active dynamic ones first, in order
@@ -431,6 +432,9 @@ RSX_F void phase5(ArenaState& S, const StaticData& D) {
     Special acc = sv.spec[i];
     emit_special(sv, S, D, acc, dt);
   }
+}
+
+RSX_F void phase5_iterate(Solver& sv) {
   // split-impulse iterations
   {
     bool run[kMaxRows];
@@ -467,6 +471,10 @@ RSX_F void phase5(ArenaState& S, const StaticData& D) {
     }
     if (lsr == 0.0f) break;
   }
+}
+
+RSX_F void phase5_finish(ArenaState& S, const StaticData& D, Solver& sv) {
+  const float dt = fdiv(1.0f, 120.0f);
   // finish
   for (int i = 0; i < sv.nb; ++i) {
     SBody& b = sv.bodies[i];
@@ -494,6 +502,13 @@ RSX_F void phase5(ArenaState& S, const StaticData& D) {
       body.deactivation_time = 0.0f;
     }
   }
+}
+
+RSX_F void phase5(ArenaState& S, const StaticData& D) {
+  Solver sv;
+  phase5_setup(S, D, sv);
+  phase5_iterate(sv);
+  phase5_finish(S, D, sv);
 }
 
 }  // namespace sim

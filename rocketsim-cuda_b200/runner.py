@@ -45,7 +45,7 @@ class DecisionRunner:
         self.Z = t.zeros((n, 8), dtype=t.float32, device=dev.device)
         self.sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
         self.pred = None
-        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 1, "threshold": None}
+        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 6, "threshold": None}
         torch.cuda.synchronize(dev.device)
 
     # ---- one decision ----
@@ -125,7 +125,7 @@ class DecisionRunner:
     # ---- the autotuner ----
     def candidates(self, binning: bool = True):
         out = []
-        for block, split in itertools.product((448, 512), (2, 3)):
+        for block, split in itertools.product((448, 512), (2, 6)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
             if binning and self.pred is not None:
                 for thr in (0.3, 0.5):
