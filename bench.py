@@ -34,7 +34,7 @@ ARENAS = 65536
 TICK_BYTES = 2567 * 4
 ALG_BYTES_PER_ARENA_TICK = (TICK_BYTES * 2 + 64 + 4) / 8.0  # state in + out, controls, result, per tick
 METRIC = "arena-ticks/s, 8-tick decision, 65,536 arenas: binned vs plain, bit-exact"
-TRAFFIC_PER_ARENA_DECISION = 4.585e9 / 32768
+TRAFFIC_PER_ARENA_DECISION = 4.709e9 / 32768
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
 
@@ -347,8 +347,8 @@ def run_ours(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 2), from the ncu capture in
-    # profiles/k_sim8_lockstep_headline.md: 4.585 GB for 32,768 arenas, scaled by the arena count
+    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 6), from the ncu capture in
+    # profiles/k_sim8_lockstep_headline.md: 4.709 GB for 32,768 arenas, scaled by the arena count
     traffic = TRAFFIC_PER_ARENA_DECISION * n if config["mode"] != "plain" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled from 32,768 arenas)",
