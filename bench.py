@@ -347,8 +347,8 @@ def run_ours(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 6), from the ncu capture in
-    # profiles/k_sim8_lockstep_headline.md: 4.709 GB for 32,768 arenas, scaled by the arena count
+    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 6), from one ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum: 4.709 GB for one 32,768-arena decision), scaled by the arena count
     traffic = TRAFFIC_PER_ARENA_DECISION * n if config["mode"] != "plain" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled from 32,768 arenas)",

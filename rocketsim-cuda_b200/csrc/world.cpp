@@ -1,5 +1,5 @@
 // Synthetic Soccar world and start states (host only).  The game's collision meshes and RocketSim V3's static dump
-// are not available, so this builds a StaticData of the reference's exact layout from a seeded synthetic arena:
+// are not available, so this file builds a StaticData of the reference's exact layout from a seeded synthetic arena:
 //   * a closed box 8192 x 10240 x 2044 uu with two goal recesses 1786 x 880 x 642 uu and quarter-cylinder fillets of
 //     radius 256 uu, every vertex jittered by +-0.5 uu from the seed, split into the 16 mesh bodies the layout has
 //     (fillets, back walls, goals and corners), the floor, ceiling and side walls as the 4 static planes;

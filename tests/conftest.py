@@ -1,8 +1,8 @@
 """Shared test setup: the `gpu` marker, the package path, and the oracle.
 
 The oracle is the reference's own correctly rounded CPU simulator (crates/rocketsim-cuda/csrc/phase.cpp over the
-reference's cuda/ headers), built from its sources by oracle/Makefile into oracle/_ref/.  Tests use it as the checker
-only; when it is absent (a machine that never had the reference sources), the committed golden fixtures of
+reference's cuda/ headers), built from its sources by oracle/Makefile into oracle/_ref/.  Tests use it to check
+against only; when it is absent (a machine that never had the reference sources), the committed golden fixtures of
 tests/golden/ stand in for it.
 """
 import ctypes

@@ -23,12 +23,12 @@ def test_modes_graphs_and_autotuner_agree(rsx):
         torch.cuda.synchronize()
         start = run.snapshot()
         run.train_predictor(control_seed=77, decisions=2, epochs=1)
-        configs = [{"mode": "plain", "block": 32},
+        modes = [{"mode": "plain", "block": 32},
                    {"mode": "lockstep", "block": 448, "grid": run.sms, "split": 1},
                    {"mode": "lockstep", "block": 64, "grid": 3, "split": 0},
                    {"mode": "binned", "block": 384, "grid": run.sms, "split": 1, "threshold": 0.3}]
         outs = []
-        for i, c in enumerate(configs):
+        for i, c in enumerate(modes):
             run.restore(start)
             if i == 1:  # as one CUDA graph of all D decisions
                 g = run.capture([x.data_ptr() for x in ctl], c)
@@ -39,9 +39,9 @@ def test_modes_graphs_and_autotuner_agree(rsx):
             run.stream.synchronize()
             outs.append((run.snapshot().cpu().numpy(), run.res.cpu().numpy().copy(), run.ev.cpu().numpy().copy()))
         for i, o in enumerate(outs[1:], 1):
-            assert np.array_equal(o[0], outs[0][0]), f"{configs[i]}: states differ"
-            assert np.array_equal(o[1], outs[0][1]), f"{configs[i]}: results differ"
-            assert np.array_equal(o[2], outs[0][2]), f"{configs[i]}: event words differ"
+            assert np.array_equal(o[0], outs[0][0]), f"{modes[i]}: states differ"
+            assert np.array_equal(o[1], outs[0][1]), f"{modes[i]}: results differ"
+            assert np.array_equal(o[2], outs[0][2]), f"{modes[i]}: event words differ"
         # the autotuner times on a snapshot and restores it
         run.restore(start)
         before = run.snapshot().cpu().numpy()
