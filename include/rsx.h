@@ -134,6 +134,11 @@ int rsx_sim8_persistent_noalloc(uint32_t* d_states, uint32_t n, const void* d_st
 int rsx_profile_phases_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                            const rsx_controls* d_controls, uint64_t* d_phase_cycles, void* stream);
 
+/* L2 residency for the static data (no counterpart in the reference): a persisting-access window over
+ * [d_ptr, d_ptr + bytes) on `stream` (bytes 0: remove it), hit_ratio in (0, 1] (scaled down when the window exceeds the
+ * device's persisting carve-out).  The carve-out is a limit of the calling process's context. */
+int rsx_l2_persist_raw(const void* d_ptr, uint64_t bytes, float hit_ratio, void* stream);
+
 /* Device resets (no counterpart in the reference): the arenas selected by d_mask (u8, nonzero: reset; null: all) and
  * by d_result (the last decision's result words; null: no condition, else only arenas whose decision scored) get the
  * start state rsx_make_states_multi builds for the same seed, arena index, StaticData and mix[5] (host memory),

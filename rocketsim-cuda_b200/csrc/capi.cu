@@ -299,6 +299,45 @@ int rsx_reset_arenas_raw(uint32_t* d_states, uint32_t n, const void* d_statics, 
   return RSX_OK;
 }
 
+// L2 residency for the static data: a persisting-access window over [d_ptr, d_ptr + bytes) on `stream` (kernels
+// launched there afterwards, and kernel nodes captured from it, keep those lines in the persisting part of L2, which
+// the streaming local-memory traffic of the decision kernels cannot evict).  bytes 0 removes the window.  The
+// persisting carve-out is a limit of this process's context: it ends with the process.
+int rsx_l2_persist_raw(const void* d_ptr, uint64_t bytes, float hit_ratio, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  RSX_CK(cudaGetDevice(&dev));
+  cudaStreamAttrValue v;
+  memset(&v, 0, sizeof(v));
+  if (bytes == 0 || !d_ptr) {
+    v.accessPolicyWindow.base_ptr = nullptr;
+    v.accessPolicyWindow.num_bytes = 0;
+    v.accessPolicyWindow.hitRatio = 0.0f;
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyNormal;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+    RSX_CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
+    return RSX_OK;
+  }
+  int max_window = 0, max_persist = 0;
+  RSX_CK(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+  RSX_CK(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
+  size_t win = bytes < (uint64_t)max_window ? (size_t)bytes : (size_t)max_window;
+  size_t carve = win < (size_t)max_persist ? win : (size_t)max_persist;
+  RSX_CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
+  v.accessPolicyWindow.base_ptr = const_cast<void*>(d_ptr);
+  v.accessPolicyWindow.num_bytes = win;
+  float hr = hit_ratio > 0.0f ? (hit_ratio < 1.0f ? hit_ratio : 1.0f) : 1.0f;
+  if (win > carve) {  // the share of the window the carve-out can hold
+    float fit = (float)carve / (float)win;
+    hr = hr < fit ? hr : fit;
+  }
+  v.accessPolicyWindow.hitRatio = hr;
+  v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  RSX_CK(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v));
+  return RSX_OK;
+}
+
 // ---- the contact predictor ----
 uint64_t rsx_pred_scratch_elems(uint32_t n) { return 2ull * (3ull * n + 16) * 128 + (uint64_t)(n + 16) * 8; }
 

@@ -97,6 +97,7 @@ def lib() -> ctypes.CDLL:
         L.rsx_sim8_lockstep_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, vp]
         L.rsx_copy_raw.argtypes = [vp, vp, ctypes.c_uint64, vp]
+        L.rsx_l2_persist_raw.argtypes = [vp, ctypes.c_uint64, ctypes.c_float, vp]
         L.rsx_reset_arenas_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), vp, vp, vp, vp]
         _lib = L
     return _lib

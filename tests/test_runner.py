@@ -30,6 +30,9 @@ def test_modes_graphs_and_autotuner_agree(rsx):
         outs = []
         for i, c in enumerate(modes):
             run.restore(start)
+            # the last mode runs with the static data in a persisting L2 window (a cache hint: same words)
+            if i == len(modes) - 1:
+                rsx.check(rsx.lib().rsx_l2_persist_raw(run.dsd.ptr(), sds.size * 4, 1.0, run.sptr), "l2 window")
             if i == 1:  # as one CUDA graph of all D decisions
                 g = run.capture([x.data_ptr() for x in ctl], c)
                 run.replay(g)
@@ -42,6 +45,7 @@ def test_modes_graphs_and_autotuner_agree(rsx):
             assert np.array_equal(o[0], outs[0][0]), f"{modes[i]}: states differ"
             assert np.array_equal(o[1], outs[0][1]), f"{modes[i]}: results differ"
             assert np.array_equal(o[2], outs[0][2]), f"{modes[i]}: event words differ"
+        rsx.check(rsx.lib().rsx_l2_persist_raw(None, 0, 0.0, run.sptr), "l2 window off")
         # the autotuner times on a snapshot and restores it
         run.restore(start)
         before = run.snapshot().cpu().numpy()
