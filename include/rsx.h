@@ -111,7 +111,8 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
  * (identity when null) from d_queue_counter (cleared by the call) when its arenas finish.  split 1 adds a barrier after
  * each car's pre-tick inside P1; split 2 splits each car's P1 into pre-tick head, wheel rays and wheel response; split 3 adds a barrier
  * after every step of P3b's pair / leaf loop; split 4 / 5 drop the barriers from P3b / P4 to P8 (slower: kept for
- * measurement); split 6 is split 2 with P5 (rows, iterations, integration) and P8 (cars, the rest) in parts.  Register budget by block: up to 384 threads 168 registers, 448 144, 512 128.  Results
+ * measurement); split 6 is split 2 with P5 (rows, iterations, integration) and P8 (cars, the rest) in parts; split 7 is
+ * split 6 with P3a one dynamic body at a time.  Register budget by block: up to 448 threads 144 registers, 512 128.  Results
  * equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
 #define RSX_LOCKSTEP_MAX_BLOCK 512u
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,

@@ -25,7 +25,6 @@ RSX_DECL_PERSIST(16)
   cudaError_t rsx_launch_sim8_lockstep_t##T(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls,         \
                                             uint32_t* result, uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n,  \
                                             uint32_t grid, uint32_t block, int split, cudaStream_t s);
-RSX_DECL_LOCKSTEP(384)
 RSX_DECL_LOCKSTEP(448)
 RSX_DECL_LOCKSTEP(512)
 cudaError_t rsx_launch_pred_features(const uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t n,
@@ -265,16 +264,13 @@ int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics,
                           uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
                           uint32_t block, uint32_t split, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
-      (block & 31) || grid == 0 || split > 6)
-    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 6");
+      (block & 31) || grid == 0 || split > 7)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 7");
   if (n == 0) return RSX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
   cudaError_t e;
-  if (block <= 384)
-    e = rsx_launch_sim8_lockstep_t384(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
-                                      block, (int)split, s);
-  else if (block <= 448)
+  if (block <= 448)
     e = rsx_launch_sim8_lockstep_t448(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
                                       block, (int)split, s);
   else

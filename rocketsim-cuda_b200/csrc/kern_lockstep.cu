@@ -7,7 +7,8 @@
 // active 4% of cycles).  Here the warps of a block step their arenas phase by phase together: a __syncthreads()
 // after each of the ten phases (split 1: also after each car's pre-tick inside P1; split 2: P1 of each car in three
 // parts, pre-tick head / wheel rays / wheel response; split 3: also a barrier after every step of P3b's pair / leaf
-// loop; split 6: split 2 with P5 as rows / iterations / integration and P8 as cars / the rest; splits 4 and 5 leave
+// loop; split 6: split 2 with P5 as rows / iterations / integration and P8 as cars / the rest; split 7: split 6 with
+// P3a one dynamic body at a time; splits 4 and 5 leave
 // the barriers out between P3b (4) or P4 (5) and P8, to measure what they buy), so that at any time the block's warps
 // fetch from one piece of code.
 //
@@ -20,8 +21,8 @@
 // stepped, the state after the first scored tick kept, event OR up to that tick), so states, result words and event
 // words equal those of every other decision kernel, whatever grid, block, split or order.
 //
-// Compiled once per register budget (RSX_LS_MAXT threads per block, one block per SM: 384 -> 168 registers,
-// 448 -> 144, 512 -> 128).
+// Compiled once per register budget (RSX_LS_MAXT threads per block, one block per SM: 448 -> 144 registers,
+// 512 -> 128).
 #include "kern_common.cuh"
 
 #ifndef RSX_LS_MAXT
@@ -105,7 +106,15 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         // split 4: no barrier between P3b and P8 (warps without contact work run ahead to the tick's end);
         // split 5: none between P4 and P8
         const bool bar = !((SPLIT == 4 && k >= 4 && k < sim::kPhases - 1) || (SPLIT == 5 && k >= 5 && k < sim::kPhases - 1));
-        if (SPLIT == 6 && k == 6) {  // P5: rows, iterations, integration
+        if (SPLIT == 7 && k == 3) {  // P3a: one dynamic body at a time
+#pragma unroll 1
+          for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
+            if (have) sim::t_p3a_body(s, *D, d);
+            __syncthreads();
+          }
+          continue;
+        }
+        if (SPLIT >= 6 && k == 6) {  // P5: rows, iterations, integration
           sim::Solver sv;
           if (have) sim::t_p5_setup(s, *D, sv);
           __syncthreads();
@@ -115,7 +124,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           __syncthreads();
           continue;
         }
-        if (SPLIT == 6 && k == 9) {  // P8: cars, then pads / ball / tick count
+        if (SPLIT >= 6 && k == 9) {  // P8: cars, then pads / ball / tick count
           if (have) sim::t_p8_cars(s);
           __syncthreads();
           if (have) sim::t_p8_rest(s, *D);
@@ -199,7 +208,9 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
                    const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split == 6)
+  if (split == 7)
+    K_NAME<7><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 6)
     K_NAME<6><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
   else if (split == 5)
     K_NAME<5><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);

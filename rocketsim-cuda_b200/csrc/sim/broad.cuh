@@ -228,12 +228,13 @@ RSX_F Box3 dyn_shape_box(const BodyConst& c, const Aff& t) {
   return c.shape == SHAPE_SPHERE ? sphere_box(c.sphere_margin, t.t) : compound_box(c, t);
 }
 
-RSX_F void phase3a(ArenaState& S, const StaticData& D) {
+// one dynamic body's swept box, sweep-and-prune update and ray-grid cells (phase3a runs the three in order)
+RSX_F void phase3a_body(ArenaState& S, const StaticData& D, uint32_t d) {
   const V3 cbt = vs(kBreakingThreshold);
-  for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
+  {
     const BodyConst& c = D.bodies[D.dyn_body[d]];
     const Body& b = S.bodies[d];
-    if (b.flags & CF_STATIC) continue;
+    if (b.flags & CF_STATIC) return;
     Box3 bx = dyn_shape_box(c, b.xf);
     bx.lo -= cbt;
     bx.hi += cbt;
@@ -260,6 +261,9 @@ RSX_F void phase3a(ArenaState& S, const StaticData& D) {
       dyn_cells_block(S, D, true, h, ni);
     }
   }
+}
+RSX_F void phase3a(ArenaState& S, const StaticData& D) {
+  for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) phase3a_body(S, D, d);
 }
 
 // ---- construction of a consistent broadphase for a fresh state (not a phase) ----

@@ -18,6 +18,7 @@ RSX_HD RSX_NOINL inline void t_p0(ArenaState& S, const StaticData& D) { phase0(S
 RSX_HD RSX_NOINL inline void t_p1(ArenaState& S, const StaticData& D) { phase1(S, D); }
 RSX_HD RSX_NOINL inline void t_p2(ArenaState& S, const StaticData& D) { phase2(S, D); }
 RSX_HD RSX_NOINL inline void t_p3a(ArenaState& S, const StaticData& D) { phase3a(S, D); }
+RSX_HD RSX_NOINL inline void t_p3a_body(ArenaState& S, const StaticData& D, uint32_t d) { phase3a_body(S, D, d); }
 RSX_HD RSX_NOINL inline uint32_t t_p3b(ArenaState& S, const StaticData& D) { return phase3b(S, D); }
 RSX_HD RSX_NOINL inline bool t_p3b_step(ArenaState& S, const StaticData& D, P3bLoop& L) { return p3b_step(S, D, L); }
 RSX_HD RSX_NOINL inline void t_p4(ArenaState& S, const StaticData& D) { phase4(S, D); }

@@ -125,7 +125,7 @@ class DecisionRunner:
     # ---- the autotuner ----
     def candidates(self, binning: bool = True):
         out = []
-        for block, split in itertools.product((448, 512), (2, 6)):
+        for block, split in itertools.product((448, 512), (6, 7)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
             if binning and self.pred is not None:
                 for thr in (0.3, 0.5):
