@@ -264,8 +264,8 @@ int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics,
                           uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
                           uint32_t block, uint32_t split, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
-      (block & 31) || grid == 0 || split > 7)
-    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 7");
+      (block & 31) || grid == 0 || split > 8)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 8");
   if (n == 0) return RSX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));

@@ -84,7 +84,17 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         bool act = false;
         float rthr = 0.0f;
         uint32_t was = 0;
-        if (have) {
+        if (SPLIT == 8) {  // the pre-tick head in three parts
+          sim::PreTick pt;
+          if (have) {
+            was = s.cars[ci].on_ground;
+            act = sim::car_pre_tick_wheels(s, *D, ci, pt);
+          }
+          __syncthreads();
+          if (have && act) sim::car_pre_tick_jumps(s, *D, ci, pt);
+          __syncthreads();
+          if (have && act) rthr = sim::car_pre_tick_air(s, *D, ci, pt);
+        } else if (have) {
           was = s.cars[ci].on_ground;
           act = sim::car_pre_tick_head(s, *D, ci, &rthr);
         }
@@ -106,7 +116,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         // split 4: no barrier between P3b and P8 (warps without contact work run ahead to the tick's end);
         // split 5: none between P4 and P8
         const bool bar = !((SPLIT == 4 && k >= 4 && k < sim::kPhases - 1) || (SPLIT == 5 && k >= 5 && k < sim::kPhases - 1));
-        if (SPLIT == 7 && k == 3) {  // P3a: one dynamic body at a time
+        if (SPLIT >= 7 && k == 3) {  // P3a: one dynamic body at a time
 #pragma unroll 1
           for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
             if (have) sim::t_p3a_body(s, *D, d);
@@ -208,7 +218,9 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
                    const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split == 7)
+  if (split == 8)
+    K_NAME<8><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+  else if (split == 7)
     K_NAME<7><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
   else if (split == 6)
     K_NAME<6><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);

@@ -651,8 +651,18 @@ RSX_F void flip_zdamp(ArenaState& S, const StaticData& D, int ci) {
 
 // The car's pre-tick up to its vehicle update; false for a demolished car (whose pre-tick ends here).  *rthr receives the
 // throttle the vehicle update uses.
-RSX_F bool car_pre_tick_head(ArenaState& S, const StaticData& D, int ci, float* rthr_out) {
-  RSX_ZONE_BEGIN(z_pre);
+// the pre-tick's values that its parts pass on
+struct PreTick {
+  float fwd, prev_ft;
+  uint32_t nwic;
+  UpCache uc;
+  bool pressed, was_jumping, prev_flipping, flip_ended;
+};
+
+// The car's pre-tick up to its vehicle update, in three parts a kernel can barrier between; part 1 returns false for a
+// demolished car (whose pre-tick ends there).
+// part 1: the demolished car's timer and respawn, else activation, control clamps and the wheels' drive and steer
+RSX_F bool car_pre_tick_wheels(ArenaState& S, const StaticData& D, int ci, PreTick& p) {
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   Body& rb = S.bodies[slot(D, cc.body)];
@@ -670,28 +680,48 @@ RSX_F bool car_pre_tick_head(ArenaState& S, const StaticData& D, int ci, float* 
   car.controls.pitch = rclamp(car.controls.pitch, -1.0f, 1.0f);
   car.controls.yaw = rclamp(car.controls.yaw, -1.0f, 1.0f);
   car.controls.roll = rclamp(car.controls.roll, -1.0f, 1.0f);
-  float fwd = fmul(dot(rb.lin_vel, rb.xf.m.c0), kBTtoUU);
-  bool pressed = car.controls.jump && !car.prev_controls.jump;
-  uint32_t nwic = wheels_in_contact(car);
-  UpCache uc = {false, vzero()};
-  update_wheels(S, D, ci, rb, fwd, uc);
+  p.fwd = fmul(dot(rb.lin_vel, rb.xf.m.c0), kBTtoUU);
+  p.pressed = car.controls.jump && !car.prev_controls.jump;
+  p.nwic = wheels_in_contact(car);
+  p.uc = UpCache{false, vzero()};
+  update_wheels(S, D, ci, rb, p.fwd, p.uc);
   if (car.on_ground) {
     if (car.is_flipping) car.flip_time = 0.0f;
     car.is_flipping = 0;
   }
-  bool was_jumping = car.is_jumping != 0;
-  update_jump(S, D, ci, rb, pressed);
-  update_auto_flip(S, D, ci, rb, pressed);
-  bool prev_flipping = car.is_flipping != 0;
-  float prev_ft = car.flip_time;
-  bool flip_ended = update_double_jump_or_flip(S, D, ci, rb, pressed, fwd, was_jumping);
-  if (!car.on_ground) update_air_torque(S, D, ci, rb, nwic, prev_flipping, prev_ft);
+  return true;
+}
+// part 2: jump, auto-flip, double jump or flip
+RSX_F void car_pre_tick_jumps(ArenaState& S, const StaticData& D, int ci, PreTick& p) {
+  Car& car = S.cars[ci];
+  Body& rb = S.bodies[slot(D, D.cars[ci].body)];
+  p.was_jumping = car.is_jumping != 0;
+  update_jump(S, D, ci, rb, p.pressed);
+  update_auto_flip(S, D, ci, rb, p.pressed);
+  p.prev_flipping = car.is_flipping != 0;
+  p.prev_ft = car.flip_time;
+  p.flip_ended = update_double_jump_or_flip(S, D, ci, rb, p.pressed, p.fwd, p.was_jumping);
+}
+// part 3: air torque, auto-roll, boost; returns the throttle the vehicle update uses
+RSX_F float car_pre_tick_air(ArenaState& S, const StaticData& D, int ci, PreTick& p) {
+  Car& car = S.cars[ci];
+  Body& rb = S.bodies[slot(D, D.cars[ci].body)];
+  if (!car.on_ground) update_air_torque(S, D, ci, rb, p.nwic, p.prev_flipping, p.prev_ft);
   float qthr = quant_axis(car.controls.throttle);
-  if (qthr != 0.0f && !car.is_flipping && !flip_ended && ((0 < nwic && nwic < 4) || car.world_contact_normal.some))
-    update_auto_roll(S, D, ci, rb, nwic, uc);
+  if (qthr != 0.0f && !car.is_flipping && !p.flip_ended && ((0 < p.nwic && p.nwic < 4) || car.world_contact_normal.some))
+    update_auto_roll(S, D, ci, rb, p.nwic, p.uc);
   car.world_contact_normal = Opt<V3>{};
   update_boost(S, D, ci, rb);
-  *rthr_out = (car.controls.boost && car.boost > 0.0f) ? 1.0f : qthr;
+  return (car.controls.boost && car.boost > 0.0f) ? 1.0f : qthr;
+}
+
+// the three parts in order; false for a demolished car.  *rthr receives the throttle the vehicle update uses.
+RSX_F bool car_pre_tick_head(ArenaState& S, const StaticData& D, int ci, float* rthr_out) {
+  RSX_ZONE_BEGIN(z_pre);
+  PreTick p;
+  if (!car_pre_tick_wheels(S, D, ci, p)) return false;
+  car_pre_tick_jumps(S, D, ci, p);
+  *rthr_out = car_pre_tick_air(S, D, ci, p);
   RSX_ZONE_END(z_pre, 0);
   return true;
 }
