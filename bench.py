@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch the timed decisions one by one instead of as CUDA graphs")
     ap.add_argument("--train-decisions", type=int, default=32, help="decisions of exact labels for the predictor")
-    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
     ap.add_argument("--split", type=int, default=6,
@@ -300,11 +300,12 @@ def run_ours(args):
     if pred_info is not None:
         run.restore(start)
         Zs, Ys = [], []
-        for s in range(steps):
-            cp = dctl[s].data_ptr()
-            run.step(cp, {"mode": "binned", "block": 448, "grid": run.sms, "split": 1, "threshold": 0.5})
-            Zs.append(run.Z.clone())
-            Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
+        with torch.cuda.stream(stream):  # the copies on the stream the kernels wrote on
+            for s in range(steps):
+                cp = dctl[s].data_ptr()
+                run.step(cp, {"mode": "binned", "block": 448, "grid": run.sms, "split": 7, "threshold": 0.5})
+                Zs.append(run.Z.clone())
+                Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         stream.synchronize()
         m = P.recall_precision(torch.cat(Zs).cpu().numpy(), torch.cat(Ys).cpu().numpy())
         pred_info["recall_precision_rate"] = {k: [round(float(x), 4) for x in v] for k, v in m.items()}

@@ -172,10 +172,11 @@ int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const
 int rsx_pred_adam_raw(float* d_w_f32, uint16_t* d_w_bf16, float* d_m, float* d_v, const float* d_grad, uint32_t step, float lr,
                       void* stream);
 int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream);
-/* Bins: arena a is contact-heavy when any of its 6 logits exceeds threshold_logit.  d_order[n] lists the heavy arenas
- * then the quiet ones, each in arena order; d_heavy_count[0] their number; d_scratch ceil(n / 1024) words. */
-int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t* d_scratch, uint32_t* d_order,
-                     uint32_t* d_heavy_count, void* stream);
+/* Bins: arena a is contact-heavy when any output in label_mask (bit k: output k; 0x3F all six) has its logit above
+ * threshold_logit.  d_order[n] lists the heavy arenas then the quiet ones, each in arena order; d_heavy_count[0] their
+ * number; d_scratch ceil(n / 1024) words. */
+int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t label_mask, uint32_t* d_scratch,
+                     uint32_t* d_order, uint32_t* d_heavy_count, void* stream);
 
 /* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
 /* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */

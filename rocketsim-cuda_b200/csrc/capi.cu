@@ -37,8 +37,8 @@ cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* sa
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
                                  float c2, cudaStream_t s);
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
-cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t* block_scratch, uint32_t* order, uint32_t* heavy_total,
-                                cudaStream_t s);
+cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
+                                uint32_t* heavy_total, cudaStream_t s);
 cudaError_t rsx_launch_reset_arenas(uint32_t* states, uint32_t n, const void* sds, const uint8_t* sd_index, uint64_t seed, const float* mix,
                                     const uint32_t* result, const uint8_t* mask, uint32_t* reset_count, cudaStream_t s);
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
@@ -393,11 +393,11 @@ int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream)
   return RSX_OK;
 }
 
-int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t* d_scratch, uint32_t* d_order, uint32_t* d_heavy_count,
-                     void* stream) {
+int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t label_mask, uint32_t* d_scratch, uint32_t* d_order,
+                     uint32_t* d_heavy_count, void* stream) {
   if (!d_logits || !d_scratch || !d_order || !d_heavy_count) return RSX_E_ARG;
   if (n == 0) return RSX_OK;
-  RSX_CK(rsx_launch_pred_bin(d_logits, n, threshold_logit, d_scratch, d_order, d_heavy_count, (cudaStream_t)stream));
+  RSX_CK(rsx_launch_pred_bin(d_logits, n, threshold_logit, label_mask, d_scratch, d_order, d_heavy_count, (cudaStream_t)stream));
   return RSX_OK;
 }
 

@@ -363,14 +363,15 @@ extern "C" __global__ void k_pred_to_bf16(const float* w, __nv_bfloat16* wb, uin
   if (i < count) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
-// ---- binning: an arena is contact-heavy when any output's logit exceeds `threshold_logit`; the order lists the
+// ---- binning: an arena is contact-heavy when any output of `mask` has its logit above `threshold_logit`; the order lists the
 // heavy arenas first (longest work first), each bin in arena order.  Two passes over blocks of 1024 arenas. ----
-extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_count(const float* logits, uint32_t n, float thr, uint32_t* block_heavy) {
+extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_count(const float* logits, uint32_t n, float thr, uint32_t mask,
+                                                                   uint32_t* block_heavy) {
   __shared__ uint32_t warp_cnt[32];
   uint32_t a = blockIdx.x * 1024 + threadIdx.x;
   bool heavy = false;
   if (a < n)
-    for (int o = 0; o < kOut; ++o) heavy |= logits[(size_t)a * kOutPad + o] > thr;
+    for (int o = 0; o < kOut; ++o) heavy |= ((mask >> o) & 1u) && logits[(size_t)a * kOutPad + o] > thr;
   uint32_t m = __ballot_sync(0xFFFFFFFFu, heavy);
   if ((threadIdx.x & 31) == 0) warp_cnt[threadIdx.x >> 5] = __popc(m);
   __syncthreads();
@@ -381,13 +382,14 @@ extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_count(const float*
   }
 }
 
-extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_scatter(const float* logits, uint32_t n, float thr, const uint32_t* block_heavy,
-                                                                     uint32_t nblocks, uint32_t* order, uint32_t* heavy_total) {
+extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_scatter(const float* logits, uint32_t n, float thr, uint32_t mask,
+                                                                     const uint32_t* block_heavy, uint32_t nblocks, uint32_t* order,
+                                                                     uint32_t* heavy_total) {
   __shared__ uint32_t warp_heavy[32], warp_quiet[32], base[2];
   uint32_t a = blockIdx.x * 1024 + threadIdx.x;
   bool live = a < n, heavy = false;
   if (live)
-    for (int o = 0; o < kOut; ++o) heavy |= logits[(size_t)a * kOutPad + o] > thr;
+    for (int o = 0; o < kOut; ++o) heavy |= ((mask >> o) & 1u) && logits[(size_t)a * kOutPad + o] > thr;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t mh = __ballot_sync(0xFFFFFFFFu, live && heavy), mq = __ballot_sync(0xFFFFFFFFu, live && !heavy);
   if (lane == 0) {
@@ -481,10 +483,10 @@ cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s) {
   k_pred_to_bf16<<<(kParams + 255) / 256, 256, 0, s>>>(w, (__nv_bfloat16*)wb, kParams);
   return cudaGetLastError();
 }
-cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t* block_scratch, uint32_t* order, uint32_t* heavy_total,
-                                cudaStream_t s) {
+cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
+                                uint32_t* heavy_total, cudaStream_t s) {
   uint32_t nb = (n + 1023) / 1024;
-  k_pred_bin_count<<<nb, 1024, 0, s>>>(logits, n, thr, block_scratch);
-  k_pred_bin_scatter<<<nb, 1024, 0, s>>>(logits, n, thr, block_scratch, nb, order, heavy_total);
+  k_pred_bin_count<<<nb, 1024, 0, s>>>(logits, n, thr, mask, block_scratch);
+  k_pred_bin_scatter<<<nb, 1024, 0, s>>>(logits, n, thr, mask, block_scratch, nb, order, heavy_total);
   return cudaGetLastError();
 }

@@ -23,6 +23,9 @@ FEATURES = 48
 LABELS = 6
 HIDDEN = 128
 PARAMS = 40328
+# outputs: 0 car 0 - ball, 1 car 1 - ball, 2 car - car, 3 ball - world, 4 car 0 - world, 5 car 1 - world
+ALL_LABELS = 0x3F
+CAR_LABELS = 0x37  # every output but ball - world
 # offsets of the parameter blocks (floats)
 OFF = {}
 _o = 0
@@ -46,7 +49,7 @@ def _bind():
     L.rsx_pred_gradients_raw.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp, vp, vp]
     L.rsx_pred_adam_raw.argtypes = [vp, vp, vp, vp, vp, u32, ctypes.c_float, vp]
     L.rsx_pred_to_bf16_raw.argtypes = [vp, vp, vp]
-    L.rsx_pred_bin_raw.argtypes = [vp, u32, ctypes.c_float, vp, vp, vp, vp]
+    L.rsx_pred_bin_raw.argtypes = [vp, u32, ctypes.c_float, u32, vp, vp, vp, vp]
     L._pred_bound = True
     return L
 
@@ -156,14 +159,15 @@ class ContactPredictor:
         return [float(l.item()) / batch for l in losses[-8:]]
 
     # ---- binning ----
-    def bin(self, Z, n: int, threshold: float = 0.5, order=None, heavy=None):
-        """Order of the arenas for the persistent kernels: predicted contact-heavy first, then quiet (each in arena order)."""
+    def bin(self, Z, n: int, threshold: float = 0.5, order=None, heavy=None, label_mask: int = 0x3F):
+        """Order of the arenas for the persistent kernels: predicted contact-heavy first (any output of label_mask above
+        the threshold), then quiet (each in arena order)."""
         t = self.torch
         order = order if order is not None else t.empty(n, dtype=t.int32, device=self.device)
         heavy = heavy if heavy is not None else t.zeros(1, dtype=t.int32, device=self.device)
         scratch = t.empty((n + 1023) // 1024, dtype=t.int32, device=self.device)
         thr = math.log(threshold / (1.0 - threshold))
-        rsx.check(self.L.rsx_pred_bin_raw(Z.data_ptr(), n, thr, scratch.data_ptr(), order.data_ptr(), heavy.data_ptr(), self.stream),
+        rsx.check(self.L.rsx_pred_bin_raw(Z.data_ptr(), n, thr, label_mask, scratch.data_ptr(), order.data_ptr(), heavy.data_ptr(), self.stream),
                   "rsx_pred_bin_raw")
         return order, heavy
 

@@ -65,8 +65,8 @@ class DecisionRunner:
                                                 self.sptr), "features")
             rsx.check(p.L.rsx_pred_forward_raw(p.wb.data_ptr(), p.w.data_ptr(), self.X.data_ptr(), n, self.Z.data_ptr(), self.sptr),
                       "forward")
-            rsx.check(p.L.rsx_pred_bin_raw(self.Z.data_ptr(), n, thr, self.bin_scratch.data_ptr(), self.order.data_ptr(),
-                                           self.heavy.data_ptr(), self.sptr), "bin")
+            rsx.check(p.L.rsx_pred_bin_raw(self.Z.data_ptr(), n, thr, c.get("labels", P.ALL_LABELS), self.bin_scratch.data_ptr(),
+                                           self.order.data_ptr(), self.heavy.data_ptr(), self.sptr), "bin")
             order = self.order.data_ptr()
         rsx.check(L.rsx_sim8_lockstep_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
                                           self.ev.data_ptr(), order, self.counter.data_ptr(), c.get("grid", self.sms), c["block"],
@@ -91,7 +91,7 @@ class DecisionRunner:
         rsx.check(rsx.lib().rsx_copy_raw(self.ds.ptr(), buf.data_ptr(), rsx.aosoa_words(self.n) * 4, self.sptr), "rsx_copy_raw")
 
     # ---- the learned part ----
-    def train_predictor(self, control_seed: int, decisions: int = 32, epochs: int = 3, seed: int = 0, lr: float = 1e-3):
+    def train_predictor(self, control_seed: int, decisions: int = 32, epochs: int = 6, seed: int = 0, lr: float = 2e-3):
         """Labels from `decisions` exact decisions of these arenas (controls of `control_seed`, run on a snapshot that is
         restored afterwards), then Adam over them; returns (samples, last losses)."""
         t = self.torch
@@ -99,7 +99,7 @@ class DecisionRunner:
             self.pred = P.ContactPredictor(self.dev.device, seed=seed, stream=self.sptr)
         snap = self.snapshot()
         Xs, Ys = [], []
-        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 1}
+        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 7}
         for d in range(decisions):
             ctl = t.from_numpy(rsx.decision_controls(control_seed, d, self.n).view(np.int32)).to(self.dev.device, non_blocking=False)
             self.stream.wait_stream(t.cuda.current_stream(self.dev.device))
@@ -128,8 +128,8 @@ class DecisionRunner:
         for block, split in itertools.product((448, 512), (6, 7)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
             if binning and self.pred is not None:
-                for thr in (0.3, 0.5):
-                    out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr})
+                for thr, labels in ((0.3, P.ALL_LABELS), (0.5, P.ALL_LABELS)):
+                    out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr, "labels": labels})
         return out
 
     def tune(self, controls_ptrs, candidates=None, repeats: int = 1):
