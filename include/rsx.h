@@ -186,6 +186,10 @@ int rsx_make_states(const uint32_t* static_words, uint32_t* states, uint32_t n, 
 /* per-arena car pairings: statics[count], sd_index[a] < count selects arena a's StaticData */
 int rsx_make_states_multi(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, uint32_t* states, uint32_t n,
                           uint64_t seed, const float* mix);
+/* the start states of chosen arenas: states[j] is arena arena_index[j]'s state for (seed, statics[sd_index[j]], mix),
+ * the words rsx_make_states_multi and the device's rsx_reset_arenas_raw give that arena */
+int rsx_make_states_at(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, const uint32_t* arena_index, uint32_t k,
+                       uint64_t seed, const float* mix, uint32_t* states);
 /* the same source compiled for the host (for debugging and CPU-side checks; the device entry points never call these) */
 int rsx_host_phase(int k, uint32_t* state_words, const uint32_t* static_words);
 uint32_t rsx_host_decide(uint32_t* state_words, const uint32_t* static_words, const rsx_controls* controls2);

@@ -5,6 +5,7 @@
 #include "../../include/rsx.h"
 #include "state.cuh"
 #include "sim/physics.cuh"
+#include "sim/start.cuh"
 
 namespace rsx {
 namespace world {
@@ -52,6 +53,17 @@ int rsx_make_states_multi(const uint32_t* statics, uint32_t count, const uint8_t
   for (uint32_t a = 0; a < n; ++a)
     if (sd_index[a] >= count) return RSX_E_ARG;
   world::make_states_multi(reinterpret_cast<const StaticData*>(statics), sd_index, reinterpret_cast<ArenaState*>(states), n, seed, mix);
+  return RSX_OK;
+}
+
+int rsx_make_states_at(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, const uint32_t* arena_index, uint32_t k,
+                       uint64_t seed, const float* mix, uint32_t* states) {
+  if (!statics || !sd_index || !arena_index || !states || !mix) return RSX_E_ARG;
+  for (uint32_t j = 0; j < k; ++j)
+    if (sd_index[j] >= count) return RSX_E_ARG;
+  const StaticData* sds = reinterpret_cast<const StaticData*>(statics);
+  ArenaState* out = reinterpret_cast<ArenaState*>(states);
+  for (uint32_t j = 0; j < k; ++j) world::make_state(sds[sd_index[j]], out[j], arena_index[j], seed, mix);
   return RSX_OK;
 }
 

@@ -97,6 +97,7 @@ def lib() -> ctypes.CDLL:
         L.rsx_sim8_lockstep_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, vp]
         L.rsx_copy_raw.argtypes = [vp, vp, ctypes.c_uint64, vp]
+        L.rsx_make_states_at.argtypes = [u32p, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), u32p]
         L.rsx_l2_persist_raw.argtypes = [vp, ctypes.c_uint64, ctypes.c_float, vp]
         L.rsx_reset_arenas_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), vp, vp, vp, vp]
         _lib = L
@@ -139,6 +140,19 @@ def make_states_multi(sds: np.ndarray, sd_index: np.ndarray, seed: int, mix: Seq
     check(lib().rsx_make_states_multi(_p(sds.reshape(-1)), sds.shape[0], idx.ctypes.data_as(ctypes.c_void_p), _p(st), n, seed, m),
           "rsx_make_states_multi")
     return st
+
+
+def make_states_at(sds: np.ndarray, sd_index: np.ndarray, arena_index: np.ndarray, seed: int, mix: Sequence[float]) -> np.ndarray:
+    """The start states of the arenas `arena_index` (their car pairings `sd_index`): the words make_states_multi and the
+    device reset give those arenas."""
+    sds = np.ascontiguousarray(sds.reshape(-1, STATIC_WORDS), dtype=np.uint32)
+    si = np.ascontiguousarray(sd_index, dtype=np.uint8)
+    ai = np.ascontiguousarray(arena_index, dtype=np.uint32)
+    out = np.zeros((ai.size, ARENA_WORDS), np.uint32)
+    m = (ctypes.c_float * 5)(*mix)
+    check(lib().rsx_make_states_at(_p(sds.reshape(-1)), sds.shape[0], si.ctypes.data_as(ctypes.c_void_p), ai.ctypes.data_as(ctypes.c_void_p),
+                                   ai.size, seed, m, _p(out)), "rsx_make_states_at")
+    return out
 
 
 def aosoa_words(n: int) -> int:
