@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="reference arm: arenas per step (0: all)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline: seconds of decisions of the workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true", help="do not sample nvidia-smi during the timed region")
     ap.add_argument("--seed", type=int, default=1)
     return ap.parse_args()
 
@@ -284,7 +285,7 @@ def run_ours(args):
             t_unb, _ = timed(unb, graph=not args.no_graph)
             modes["lockstep_unbinned"] = world_size * n * 8 * args.steps / (t_unb / 1e3)
     clk = Clocks(local)
-    t_ms, ms_steps = timed(config, graph=not args.no_graph and config["mode"] != "plain", clk=clk)
+    t_ms, ms_steps = timed(config, graph=not args.no_graph and config["mode"] != "plain", clk=None if args.no_clocks else clk)
     value = world_size * n * 8 * args.steps / (t_ms / 1e3)
     modes[config["mode"]] = value
     words_tuned = run.snapshot()
