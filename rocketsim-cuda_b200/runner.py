@@ -124,7 +124,8 @@ class DecisionRunner:
 
     # ---- the autotuner ----
     def candidates(self, binning: bool = True):
-        out = []
+        # the plain launch too: with few arenas per SM (a few thousand arenas) the barriers cost more than they save
+        out = [{"mode": "plain", "block": 32}, {"mode": "plain", "block": 64}]
         for block, split in itertools.product((448, 512), (6, 7)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
             if binning and self.pred is not None:
