@@ -21,6 +21,7 @@ extern "C" {
 #define RSX_E_CUDA (-2)     /* a CUDA runtime error (rsx_last_error() names it) */
 #define RSX_E_NODEV (-3)    /* no CUDA device / no sm_100 device */
 #define RSX_E_TIMEOUT (-4)  /* a bounded device wait gave up (persistent kernel) */
+#define RSX_E_FORMAT (-5)   /* a V3 dump that does not import (rsx_last_error() says why, in the reference's words) */
 
 /* ---- constants (device.rs:16-28, arena_step.cuh:16-18) ---- */
 #define RSX_TICKS_PER_DECISION 8u
@@ -193,6 +194,39 @@ int rsx_make_states_at(const uint32_t* statics, uint32_t count, const uint8_t* s
 /* the same source compiled for the host (for debugging and CPU-side checks; the device entry points never call these) */
 int rsx_host_phase(int k, uint32_t* state_words, const uint32_t* static_words);
 uint32_t rsx_host_decide(uint32_t* state_words, const uint32_t* static_words, const rsx_controls* controls2);
+
+/* ---- V3 dumps (crates/rocketsim-cuda/src/dump.rs:1-1300; the V3 side: v3/rocketsim-dump.patch, src/dump.rs) ----
+ * Import and export of the per-arena state ("V3ARENA\0" version 2) and the static collision data ("V3STATIC"
+ * version 3, FNV-1a 64 over its payload) that the patched RocketSim V3 writes.  Host functions; buffers are the
+ * caller's.  A write returns RSX_E_ARG with the size it needs in *len when out is NULL or cap is short.  An import
+ * that the reference refuses (a list over its cap, another game mode's state, constants that differ from StaticData,
+ * a truncated or trailing dump) returns RSX_E_FORMAT with the reference's message in rsx_last_error(). */
+#define RSX_V3_ARENA_HEADER_LEN 68u   /* magic, version, config hash, 12 u32 counts (dump.rs:18) */
+#define RSX_V3_STATIC_HEADER_LEN 76u  /* magic, version, payload hash, payload length, 12 u32 counts (dump.rs:19) */
+#define RSX_V3_BODY_RECORD_LEN 219u   /* one BODY record (dump.rs:21) */
+/* What an ArenaState leaves out of a V3 arena dump (dump.rs:209-238, Template): the config hash, the BODY records of
+ * the static bodies, the sweep-and-prune counters, the manifold table stride and the other modes' ball info. */
+typedef struct rsx_v3_template {
+  uint64_t config_hash;
+  uint8_t static_body[23][RSX_V3_BODY_RECORD_LEN];
+  uint16_t num_handles, next_new_handle;
+  uint32_t manifold_stride;
+  uint8_t ball_other[24];
+  uint32_t ball_other_set;
+} rsx_v3_template;
+uint64_t rsx_v3_fnv1a64(const uint8_t* bytes, size_t len);                          /* dump.rs:30-36 */
+int rsx_v3_parse_static(const uint8_t* bytes, size_t len, uint32_t* static_words);  /* parse_static, dump.rs:976-1012 */
+/* the static dump of a StaticData (the V3 side's export_static layout); the reference only reads these */
+int rsx_v3_write_static(const uint32_t* static_words, uint8_t* out, size_t cap, size_t* len);
+/* config_hash of a StaticData: FNV-1a over its static dump's WRLD, BODY, PLAN, CARS and PADS sections */
+int rsx_v3_config_hash(const uint32_t* static_words, uint64_t* hash);
+/* a template for a StaticData without a V3 dump (unmoving, unrotated static bodies) */
+int rsx_v3_template_init(const uint32_t* static_words, rsx_v3_template* t);
+/* parse_arena (dump.rs:884-900): one arena dump into 2784 state words and its template */
+int rsx_v3_parse_arena(const uint8_t* bytes, size_t len, const uint32_t* static_words, uint32_t* state_words, rsx_v3_template* t);
+/* write_arena (dump.rs:902-944) */
+int rsx_v3_write_arena(const uint32_t* state_words, const uint32_t* static_words, const rsx_v3_template* t, uint8_t* out, size_t cap,
+                       size_t* len);
 
 /* ---- verification of the FP64-free correctly rounded libm (sin, cos, tan, atan2, pow and the auto-flip helpers) ----
  * fn 0 sin, 1 cos, 2 tan, 3 atan2(a, b), 4 pow(a, b), 5 float(double atan2(a, b)), 6 float(double hypot(a, b)) */

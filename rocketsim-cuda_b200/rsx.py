@@ -100,8 +100,25 @@ def lib() -> ctypes.CDLL:
         L.rsx_make_states_at.argtypes = [u32p, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), u32p]
         L.rsx_l2_persist_raw.argtypes = [vp, ctypes.c_uint64, ctypes.c_float, vp]
         L.rsx_reset_arenas_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), vp, vp, vp, vp]
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        tp = ctypes.POINTER(V3Template)
+        L.rsx_v3_fnv1a64.argtypes = [vp, ctypes.c_size_t]
+        L.rsx_v3_fnv1a64.restype = ctypes.c_uint64
+        L.rsx_v3_parse_static.argtypes = [vp, ctypes.c_size_t, u32p]
+        L.rsx_v3_write_static.argtypes = [u32p, vp, ctypes.c_size_t, szp]
+        L.rsx_v3_config_hash.argtypes = [u32p, ctypes.POINTER(ctypes.c_uint64)]
+        L.rsx_v3_template_init.argtypes = [u32p, tp]
+        L.rsx_v3_parse_arena.argtypes = [vp, ctypes.c_size_t, u32p, u32p, tp]
+        L.rsx_v3_write_arena.argtypes = [u32p, u32p, tp, vp, ctypes.c_size_t, szp]
         _lib = L
     return _lib
+
+
+class V3Template(ctypes.Structure):
+    """What an ArenaState leaves out of a V3 arena dump (rsx_v3_template; the reference's dump.rs Template)."""
+    _fields_ = [("config_hash", ctypes.c_uint64), ("static_body", (ctypes.c_uint8 * 219) * 23), ("num_handles", ctypes.c_uint16),
+                ("next_new_handle", ctypes.c_uint16), ("manifold_stride", ctypes.c_uint32), ("ball_other", ctypes.c_uint8 * 24),
+                ("ball_other_set", ctypes.c_uint32)]
 
 
 def _p(a: np.ndarray):
@@ -153,6 +170,73 @@ def make_states_at(sds: np.ndarray, sd_index: np.ndarray, arena_index: np.ndarra
     check(lib().rsx_make_states_at(_p(sds.reshape(-1)), sds.shape[0], si.ctypes.data_as(ctypes.c_void_p), ai.ctypes.data_as(ctypes.c_void_p),
                                    ai.size, seed, m, _p(out)), "rsx_make_states_at")
     return out
+
+
+# ---- V3 dumps (the reference's crates/rocketsim-cuda/src/dump.rs) ------------------------------------------------
+E_FORMAT = -5
+
+
+def _bytes_arg(b: bytes):
+    buf = ctypes.create_string_buffer(bytes(b), len(b))
+    return buf, len(b)
+
+
+def _write_out(fn, *args) -> bytes:
+    n = ctypes.c_size_t(0)
+    fn(*args, None, 0, ctypes.byref(n))  # asks for the size
+    out = ctypes.create_string_buffer(n.value)
+    check(fn(*args, out, n.value, ctypes.byref(n)), fn.__name__)
+    return out.raw[:n.value]
+
+
+def v3_fnv1a64(b: bytes) -> int:
+    buf, n = _bytes_arg(b)
+    return int(lib().rsx_v3_fnv1a64(buf, n))
+
+
+def v3_parse_static(b: bytes) -> np.ndarray:
+    """A V3STATIC (version 3) dump as StaticData words (parse_static)."""
+    buf, n = _bytes_arg(b)
+    sd = np.zeros(STATIC_WORDS, np.uint32)
+    check(lib().rsx_v3_parse_static(buf, n, _p(sd)), "rsx_v3_parse_static")
+    return sd
+
+
+def v3_write_static(sd: np.ndarray) -> bytes:
+    sd = np.ascontiguousarray(sd, np.uint32)
+    return _write_out(lib().rsx_v3_write_static, _p(sd))
+
+
+def v3_config_hash(sd: np.ndarray) -> int:
+    sd = np.ascontiguousarray(sd, np.uint32)
+    h = ctypes.c_uint64(0)
+    check(lib().rsx_v3_config_hash(_p(sd), ctypes.byref(h)), "rsx_v3_config_hash")
+    return int(h.value)
+
+
+def v3_template(sd: np.ndarray) -> V3Template:
+    """A template for a StaticData without a V3 dump (the synthetic world)."""
+    sd = np.ascontiguousarray(sd, np.uint32)
+    t = V3Template()
+    check(lib().rsx_v3_template_init(_p(sd), ctypes.byref(t)), "rsx_v3_template_init")
+    return t
+
+
+def v3_parse_arena(b: bytes, sd: np.ndarray):
+    """A V3ARENA (version 2) dump as 2784 state words, and its template (parse_arena)."""
+    sd = np.ascontiguousarray(sd, np.uint32)
+    buf, n = _bytes_arg(b)
+    st = np.zeros(ARENA_WORDS, np.uint32)
+    t = V3Template()
+    check(lib().rsx_v3_parse_arena(buf, n, _p(sd), _p(st), ctypes.byref(t)), "rsx_v3_parse_arena")
+    return st, t
+
+
+def v3_write_arena(state: np.ndarray, sd: np.ndarray, t: V3Template) -> bytes:
+    """An ArenaState as a V3 arena dump (write_arena)."""
+    state = np.ascontiguousarray(state, np.uint32)
+    sd = np.ascontiguousarray(sd, np.uint32)
+    return _write_out(lib().rsx_v3_write_arena, _p(state), _p(sd), ctypes.byref(t))
 
 
 def aosoa_words(n: int) -> int:
