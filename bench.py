@@ -35,6 +35,10 @@ TICK_BYTES = 2567 * 4
 ALG_BYTES_PER_ARENA_TICK = (TICK_BYTES * 2 + 64 + 4) / 8.0  # state in + out, controls, result, per tick
 METRIC = "arena-ticks/s, 8-tick decision, 65,536 arenas: binned vs plain, bit-exact"
 TRAFFIC_PER_ARENA_DECISION = 4.709e9 / 32768
+# k_observe: 171 state words read (ball 9, tick 2, pads 102, both cars' 29), result + event OR + pairing index 9 bytes,
+# two 208-byte FP16 rows and two FP32 rewards written
+OBS_BYTES_PER_ARENA = 171 * 4 + 9 + 2 * 208 + 2 * 4
+OBS_REPS = 20
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
 
@@ -338,6 +342,19 @@ def run_ours(args):
     r = pin_res.numpy().view(np.uint32)
     flags = {"scored": int(((r & 0xFF) != 0).sum()), "overflow": int(((r >> 30) & 1).sum()), "unimplemented": int((r >> 31).sum())}
 
+    # ---- observations and rewards after the decision (k_observe), timed alone on the same states ----
+    weights = [10.0, 0.5, 0.25, 2.0, -2.0, 0.125, 0.01, 0.02]
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            run.observe(weights)
+        o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        o0.record(stream)
+        for _ in range(OBS_REPS):
+            run.observe(weights)
+        o1.record(stream)
+        o1.synchronize()
+    obs_ms = reduce_max(o0.elapsed_time(o1)) / OBS_REPS
+
     # ---- roofline of the decision kernel (HBM: algorithmic bytes per launch / launch time) ----
     mean_ms = t_ms / args.steps
     alg_bytes = n * 8 * ALG_BYTES_PER_ARENA_TICK
@@ -356,6 +373,11 @@ def run_ours(args):
                 "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled from 32,768 arenas)",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": mean_ms}
+
+    observe = {"kernel": "k_observe", "ms_per_launch": obs_ms, "arenas": n,
+               "achieved_gbs": OBS_BYTES_PER_ARENA * n / (obs_ms / 1e3) / 1e9,
+               "frac": OBS_BYTES_PER_ARENA * n / (obs_ms / 1e3) / 1e9 / peak, "bytes_per_arena": OBS_BYTES_PER_ARENA,
+               "share_of_decision": obs_ms / mean_ms}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -387,6 +409,7 @@ def run_ours(args):
             "predictor": pred_info,
             "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * 4},
             "roofline": roofline,
+            "observe": observe,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": run.kernels_per_step(config) * args.steps,

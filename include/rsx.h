@@ -179,6 +179,27 @@ int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream)
 int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t label_mask, uint32_t* d_scratch,
                      uint32_t* d_order, uint32_t* d_heavy_count, void* stream);
 
+/* ---- observations and rewards for a learner (no counterpart in the reference, which defines no observation; its
+ * FP16 conversion, cuda/common/hd.cuh:167-176, is the rounding used: nearest even, as cvt.rn.f16.f32) ----
+ * After a decision, per arena a and car c (row 2a + c): RSX_OBS_DIM FP16 values, seen from c's side (car 1's x and y
+ * negated, its pads in mirrored order), positions and velocities / 2300, angular velocities / pi, boost / 100:
+ *   [0,9) ball position, velocity, angular velocity; [9,24) own position, forward (rotation x axis), up (z axis),
+ *   velocity, angular velocity; [24] boost; [25..29] on ground, has jumped, has double jumped, has flipped, demoed;
+ *   [30,36) ball minus own position and velocity; [36,51) opponent position, forward, up, velocity, angular velocity;
+ *   [51..53] opponent boost, on ground, demoed; [54,60) opponent minus own position and velocity; [60,68) own
+ *   controls (5 axes, jump, boost, handbrake as 0/1); [68,102) boost pads active (the game's cooldown test) 0/1;
+ *   [102,104) zero.
+ * Reward per car: sum over k of weights[k] * term[k] (FP32, k ascending): goal (+1 own team scored, -1 conceded, from
+ * the result word and the ball's side), ball touch, bump given, demo given, demoed, boost pickup (the decision's event
+ * OR; 0 without it), own velocity toward the ball / 2300, ball velocity toward the opponent's goal / 2300.
+ * d_obs must be 16-byte aligned; d_pad_mirror (count x 34 bytes from rsx_pad_mirror) and d_reward may be NULL. */
+#define RSX_OBS_DIM 104u
+#define RSX_REWARD_TERMS 8u
+int rsx_pad_mirror(const uint32_t* statics, uint32_t count, uint8_t* out);
+int rsx_observe_raw(const uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const uint8_t* d_pad_mirror,
+                    const uint32_t* d_result, const uint32_t* d_event_or, const float* weights, uint16_t* d_obs, float* d_reward,
+                    void* stream);
+
 /* ---- host side: the synthetic world and seeded start states (the game's meshes and V3's dumps are absent) ---- */
 /* builds one StaticData (317,895 words) for the car pairing (preset0, preset1), presets 0..6; returns the triangle count */
 int rsx_build_static(uint32_t* words, uint64_t seed, int preset0, int preset1);

@@ -39,6 +39,9 @@ cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const f
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
                                 uint32_t* heavy_total, cudaStream_t s);
+cudaError_t rsx_launch_observe(const uint32_t* states, uint32_t n, const void* sds, const uint8_t* sd_index, const uint8_t* pad_mirror,
+                               const uint32_t* result, const uint32_t* event_or, const float* weights, uint16_t* obs, float* reward,
+                               cudaStream_t s);
 cudaError_t rsx_launch_reset_arenas(uint32_t* states, uint32_t n, const void* sds, const uint8_t* sd_index, uint64_t seed, const float* mix,
                                     const uint32_t* result, const uint8_t* mask, uint32_t* reset_count, cudaStream_t s);
 cudaError_t rsx_launch_identity(const uint32_t* in, uint32_t* out, uint32_t n, int tick_only, cudaStream_t s);
@@ -292,6 +295,16 @@ int rsx_reset_arenas_raw(uint32_t* d_states, uint32_t n, const void* d_statics, 
   if (!d_states || !d_statics || !mix) return RSX_E_ARG;
   if (n == 0) return RSX_OK;
   RSX_CK(rsx_launch_reset_arenas(d_states, n, d_statics, d_sd_index, seed, mix, d_result, d_mask, d_reset_count, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_observe_raw(const uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const uint8_t* d_pad_mirror,
+                    const uint32_t* d_result, const uint32_t* d_event_or, const float* weights, uint16_t* d_obs, float* d_reward, void* stream) {
+  if (!d_states || !d_statics || !d_obs || ((uintptr_t)d_obs & 15u) != 0)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_observe_raw: null buffer or an observation buffer not 16-byte aligned");
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_observe(d_states, n, d_statics, d_sd_index, d_pad_mirror, d_result, d_event_or, weights, d_obs, d_reward,
+                            (cudaStream_t)stream));
   return RSX_OK;
 }
 

@@ -56,6 +56,24 @@ int rsx_make_states_multi(const uint32_t* statics, uint32_t count, const uint8_t
   return RSX_OK;
 }
 
+int rsx_pad_mirror(const uint32_t* statics, uint32_t count, uint8_t* out) {
+  if (!statics || !out) return RSX_E_ARG;
+  for (uint32_t k = 0; k < count; ++k) {
+    const StaticData& sd = reinterpret_cast<const StaticData*>(statics)[k];
+    for (int p = 0; p < kPads; ++p) {
+      const V3 m = V3{-sd.pads[p].pos.x, -sd.pads[p].pos.y, sd.pads[p].pos.z};
+      int q = p;  // a pad with no mirror image keeps its own place
+      for (int j = 0; j < kPads; ++j)
+        if (sd.pads[j].pos.x == m.x && sd.pads[j].pos.y == m.y && sd.pads[j].pos.z == m.z) {
+          q = j;
+          break;
+        }
+      out[(size_t)k * kPads + p] = (uint8_t)q;
+    }
+  }
+  return RSX_OK;
+}
+
 int rsx_make_states_at(const uint32_t* statics, uint32_t count, const uint8_t* sd_index, const uint32_t* arena_index, uint32_t k,
                        uint64_t seed, const float* mix, uint32_t* states) {
   if (!statics || !sd_index || !arena_index || !states || !mix) return RSX_E_ARG;

@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
         L.rsx_make_states_at.argtypes = [u32p, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), u32p]
         L.rsx_l2_persist_raw.argtypes = [vp, ctypes.c_uint64, ctypes.c_float, vp]
         L.rsx_reset_arenas_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), vp, vp, vp, vp]
+        L.rsx_pad_mirror.argtypes = [u32p, ctypes.c_uint32, vp]
+        L.rsx_observe_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_float), vp, vp, vp]
         szp = ctypes.POINTER(ctypes.c_size_t)
         tp = ctypes.POINTER(V3Template)
         L.rsx_v3_fnv1a64.argtypes = [vp, ctypes.c_size_t]
@@ -169,6 +171,19 @@ def make_states_at(sds: np.ndarray, sd_index: np.ndarray, arena_index: np.ndarra
     m = (ctypes.c_float * 5)(*mix)
     check(lib().rsx_make_states_at(_p(sds.reshape(-1)), sds.shape[0], si.ctypes.data_as(ctypes.c_void_p), ai.ctypes.data_as(ctypes.c_void_p),
                                    ai.size, seed, m, _p(out)), "rsx_make_states_at")
+    return out
+
+
+OBS_DIM = 104
+REWARD_TERMS = 8
+
+
+def pad_mirror(sds: np.ndarray) -> np.ndarray:
+    """For each StaticData, the pad at the mirror image (-x, -y, z) of each pad (count x 34 u8): car 1's pad order in
+    its observation."""
+    sds = np.ascontiguousarray(sds.reshape(-1, STATIC_WORDS), np.uint32)
+    out = np.zeros((sds.shape[0], 34), np.uint8)
+    check(lib().rsx_pad_mirror(_p(sds.reshape(-1)), sds.shape[0], out.ctypes.data_as(ctypes.c_void_p)), "rsx_pad_mirror")
     return out
 
 

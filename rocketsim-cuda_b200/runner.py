@@ -13,6 +13,7 @@ time alone; `tune()` restores the same start states before each candidate so tha
 """
 from __future__ import annotations
 
+import ctypes
 import itertools
 
 import numpy as np
@@ -30,6 +31,7 @@ class DecisionRunner:
         self.n = states.shape[0]
         self.stream = stream if stream is not None else torch.cuda.Stream(device=dev.device)
         self.sptr = self.stream.cuda_stream
+        self.statics_host = np.ascontiguousarray(statics.reshape(-1, rsx.STATIC_WORDS), np.uint32)
         self.dsd = dev.upload_static(statics)
         self.ds = dev.upload_states(states)
         n = self.n
@@ -47,6 +49,22 @@ class DecisionRunner:
         self.pred = None
         self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 6, "threshold": None}
         torch.cuda.synchronize(dev.device)
+
+    # ---- observations and rewards of the last decision ----
+    def observe(self, weights) -> tuple:
+        """Launches rsx_observe_raw on the runner's stream over the current states, the last decision's result words
+        and event OR: returns (obs (2n, 104) int16 holding FP16 bits, reward (2n,) float32), device tensors reused by
+        later calls."""
+        t = self.torch
+        if not hasattr(self, "obs"):
+            self.obs = t.zeros((2 * self.n, rsx.OBS_DIM), dtype=t.int16, device=self.dev.device)
+            self.reward = t.zeros(2 * self.n, dtype=t.float32, device=self.dev.device)
+            self.mirror = t.from_numpy(rsx.pad_mirror(self.statics_host).reshape(-1)).to(self.dev.device)
+        w = (ctypes.c_float * rsx.REWARD_TERMS)(*[float(x) for x in weights])
+        rsx.check(rsx.lib().rsx_observe_raw(self.ds.ptr(), self.n, self.dsd.ptr(), self.didx.data_ptr(), self.mirror.data_ptr(),
+                                            self.res.data_ptr(), self.ev.data_ptr(), w, self.obs.data_ptr(), self.reward.data_ptr(),
+                                            self.sptr), "rsx_observe_raw")
+        return self.obs, self.reward
 
     # ---- one decision ----
     def step(self, controls_ptr: int, config: dict | None = None) -> None:
