@@ -34,10 +34,11 @@ ARENAS = 65536
 TICK_BYTES = 2567 * 4
 ALG_BYTES_PER_ARENA_TICK = (TICK_BYTES * 2 + 64 + 4) / 8.0  # state in + out, controls, result, per tick
 METRIC = "arena-ticks/s, 8-tick decision, 65,536 arenas: binned vs plain, bit-exact"
-TRAFFIC_PER_ARENA_DECISION = 4.709e9 / 32768
-# k_observe: 171 state words read (ball 9, tick 2, pads 102, both cars' 29), result + event OR + pairing index 9 bytes,
-# two 208-byte FP16 rows and two FP32 rewards written
-OBS_BYTES_PER_ARENA = 171 * 4 + 9 + 2 * 208 + 2 * 4
+TRAFFIC_PER_ARENA_DECISION = 4.716e9 / 32768
+# k_observe: 103 state words always read (ball 9, tick 2, the 34 pads' "gave boost" flags, both cars' 29; a pad's tick
+# words only when its flag is set), result + event OR + pairing index 9 bytes, two 208-byte FP16 rows and two FP32
+# rewards written
+OBS_BYTES_PER_ARENA = 103 * 4 + 9 + 2 * 208 + 2 * 4
 OBS_REPS = 20
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
@@ -366,8 +367,8 @@ def run_ours(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 6), from one ncu capture
-    # (dram__bytes_read.sum + dram__bytes_write.sum: 4.709 GB for one 32,768-arena decision), scaled by the arena count
+    # DRAM bytes (read + write) per arena-decision of the lockstep kernel (block 448, split 7), from one ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum: 4.716 GB for one 32,768-arena decision), scaled by the arena count
     traffic = TRAFFIC_PER_ARENA_DECISION * n if config["mode"] != "plain" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, scaled from 32,768 arenas)",
