@@ -284,7 +284,7 @@ def run_ours(args):
     if not args.no_plain and config["mode"] != "plain":
         t_plain, _ = timed({"mode": "plain", "block": args.plain_block})
         modes["plain"] = world_size * n * 8 * args.steps / (t_plain / 1e3)
-    if config["mode"] == "binned" and tune_top:
+    if config["mode"] in ("binned", "levels") and tune_top:
         unb = next((c for c in [dict(c) for _, c in tuned] if c["mode"] == "lockstep"), None)
         if unb:
             t_unb, _ = timed(unb, graph=not args.no_graph)

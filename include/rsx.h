@@ -178,6 +178,12 @@ int rsx_pred_to_bf16_raw(const float* d_w_f32, uint16_t* d_w_bf16, void* stream)
  * number; d_scratch ceil(n / 1024) words. */
 int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, uint32_t label_mask, uint32_t* d_scratch,
                      uint32_t* d_order, uint32_t* d_heavy_count, void* stream);
+/* Cost levels: e = sum_k weights[k] * sigmoid(logit_k) over the six outputs (weights: 6 host floats), quantised to
+ * `levels` (2..32) levels of e / max(e) over the batch; d_order[n] lists the arenas by level, highest first, each level
+ * in arena order.  d_scratch 1 + levels * ceil(n / 1024) words.  With several claim rounds of the lockstep kernel
+ * (more arenas than its threads), the costliest arenas start first. */
+int rsx_pred_levels_raw(const float* d_logits, uint32_t n, const float* weights, uint32_t levels, uint32_t* d_scratch, uint32_t* d_order,
+                        void* stream);
 
 /* ---- observations and rewards for a learner (no counterpart in the reference, which defines no observation; its
  * FP16 conversion, cuda/common/hd.cuh:167-176, is the rounding used: nearest even, as cvt.rn.f16.f32) ----

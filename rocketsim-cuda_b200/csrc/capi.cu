@@ -37,6 +37,8 @@ cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* sa
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
                                  float c2, cudaStream_t s);
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
+cudaError_t rsx_launch_pred_levels(const float* logits, uint32_t n, const float* weights, int levels, uint32_t* scratch, uint32_t* order,
+                                   cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
                                 uint32_t* heavy_total, cudaStream_t s);
 cudaError_t rsx_launch_observe(const uint32_t* states, uint32_t n, const void* sds, const uint8_t* sd_index, const uint8_t* pad_mirror,
@@ -411,6 +413,15 @@ int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, u
   if (!d_logits || !d_scratch || !d_order || !d_heavy_count) return RSX_E_ARG;
   if (n == 0) return RSX_OK;
   RSX_CK(rsx_launch_pred_bin(d_logits, n, threshold_logit, label_mask, d_scratch, d_order, d_heavy_count, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_levels_raw(const float* d_logits, uint32_t n, const float* weights, uint32_t levels, uint32_t* d_scratch, uint32_t* d_order,
+                        void* stream) {
+  if (!d_logits || !weights || !d_scratch || !d_order || levels < 2 || levels > 32)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_pred_levels_raw: null buffer or levels outside 2..32");
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_levels(d_logits, n, weights, (int)levels, d_scratch, d_order, (cudaStream_t)stream));
   return RSX_OK;
 }
 

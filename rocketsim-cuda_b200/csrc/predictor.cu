@@ -418,6 +418,80 @@ extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_scatter(const floa
   order[heavy ? hb + __popc(mh & below) : qb + __popc(mq & below)] = a;
 }
 
+// ---- cost levels: an arena's expected contact count e = sum_k w_k * sigmoid(logit_k) over the six outputs, quantised
+// to `levels` levels of e / max(e) (the maximum over this batch); the order lists the arenas by level, highest first,
+// each level in arena order (a stable counting sort).  Three passes over blocks of 1024 arenas: the maximum, per-block
+// level counts, then the scatter. ----
+constexpr int kMaxLevels = 32;
+struct LevelWeights {
+  float w[kOut];
+};
+__device__ __forceinline__ float expected_contacts(const float* logits, uint32_t a, const LevelWeights& lw) {
+  float e = 0.0f;
+  for (int o = 0; o < kOut; ++o) e += lw.w[o] / (1.0f + expf(-logits[(size_t)a * kOutPad + o]));
+  return e;
+}
+__device__ __forceinline__ int level_of(float e, float emax, int levels) {
+  if (!(emax > 0.0f)) return 0;
+  int l = (int)(e / emax * (float)levels);
+  return l < 0 ? 0 : (l >= levels ? levels - 1 : l);
+}
+
+extern "C" __global__ void __launch_bounds__(1024) k_pred_level_max(const float* logits, uint32_t n, LevelWeights lw, uint32_t* emax_bits) {
+  uint32_t a = blockIdx.x * 1024 + threadIdx.x;
+  float e = a < n ? expected_contacts(logits, a, lw) : 0.0f;
+  for (int d = 16; d > 0; d >>= 1) e = fmaxf(e, __shfl_xor_sync(0xFFFFFFFFu, e, d));
+  if ((threadIdx.x & 31) == 0 && e > 0.0f) atomicMax(emax_bits, __float_as_uint(e));  // non-negative floats order as integers
+}
+
+extern "C" __global__ void __launch_bounds__(1024) k_pred_level_count(const float* logits, uint32_t n, LevelWeights lw, int levels,
+                                                                     const uint32_t* emax_bits, uint32_t* block_hist) {
+  __shared__ uint32_t hist[kMaxLevels];
+  if (threadIdx.x < kMaxLevels) hist[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t a = blockIdx.x * 1024 + threadIdx.x;
+  if (a < n) atomicAdd(&hist[level_of(expected_contacts(logits, a, lw), __uint_as_float(*emax_bits), levels)], 1u);
+  __syncthreads();
+  if (threadIdx.x < (uint32_t)levels) block_hist[(size_t)blockIdx.x * levels + threadIdx.x] = hist[threadIdx.x];
+}
+
+extern "C" __global__ void __launch_bounds__(1024) k_pred_level_scatter(const float* logits, uint32_t n, LevelWeights lw, int levels,
+                                                                       const uint32_t* emax_bits, const uint32_t* block_hist,
+                                                                       uint32_t nblocks, uint32_t* order) {
+  __shared__ uint32_t total[kMaxLevels], before[kMaxLevels], base[kMaxLevels], warp_cnt[32][kMaxLevels];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x < (uint32_t)levels) {
+    uint32_t t = 0, b = 0;
+    for (uint32_t k = 0; k < nblocks; ++k) {
+      uint32_t c = block_hist[(size_t)k * levels + threadIdx.x];
+      t += c;
+      if (k < blockIdx.x) b += c;
+    }
+    total[threadIdx.x] = t;
+    before[threadIdx.x] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x < (uint32_t)levels) {
+    uint32_t higher = 0;  // arenas of the levels above, which come first
+    for (int l = levels - 1; l > (int)threadIdx.x; --l) higher += total[l];
+    base[threadIdx.x] = higher + before[threadIdx.x];
+  }
+  const uint32_t a = blockIdx.x * 1024 + threadIdx.x;
+  const bool live = a < n;
+  const int lv = live ? level_of(expected_contacts(logits, a, lw), __uint_as_float(*emax_bits), levels) : -1;
+  uint32_t mine = 0;
+  for (int l = 0; l < levels; ++l) {
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, lv == l);
+    if (lane == 0) warp_cnt[warp][l] = __popc(m);
+    if (lv == l) mine = m;
+  }
+  __syncthreads();
+  if (!live) return;
+  uint32_t at = base[lv];
+  for (uint32_t w = 0; w < warp; ++w) at += warp_cnt[w][lv];
+  order[at + __popc(mine & ((1u << lane) - 1u))] = a;
+}
+
 // ---- launchers ----
 static size_t pred_smem() { return sizeof(Smem); }
 
@@ -481,6 +555,18 @@ cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const f
 }
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s) {
   k_pred_to_bf16<<<(kParams + 255) / 256, 256, 0, s>>>(w, (__nv_bfloat16*)wb, kParams);
+  return cudaGetLastError();
+}
+cudaError_t rsx_launch_pred_levels(const float* logits, uint32_t n, const float* weights, int levels, uint32_t* scratch, uint32_t* order,
+                                   cudaStream_t s) {
+  LevelWeights lw;
+  for (int o = 0; o < kOut; ++o) lw.w[o] = weights[o];
+  const uint32_t nb = (n + 1023) / 1024;
+  cudaError_t e = cudaMemsetAsync(scratch, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  k_pred_level_max<<<nb, 1024, 0, s>>>(logits, n, lw, scratch);
+  k_pred_level_count<<<nb, 1024, 0, s>>>(logits, n, lw, levels, scratch, scratch + 1);
+  k_pred_level_scatter<<<nb, 1024, 0, s>>>(logits, n, lw, levels, scratch, scratch + 1, nb, order);
   return cudaGetLastError();
 }
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,

@@ -50,6 +50,7 @@ def _bind():
     L.rsx_pred_adam_raw.argtypes = [vp, vp, vp, vp, vp, u32, ctypes.c_float, vp]
     L.rsx_pred_to_bf16_raw.argtypes = [vp, vp, vp]
     L.rsx_pred_bin_raw.argtypes = [vp, u32, ctypes.c_float, u32, vp, vp, vp, vp]
+    L.rsx_pred_levels_raw.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32, vp, vp, vp]
     L._pred_bound = True
     return L
 

@@ -43,6 +43,7 @@ class DecisionRunner:
         self.order = t.zeros(n, dtype=t.int32, device=dev.device)
         self.heavy = t.zeros(1, dtype=t.int32, device=dev.device)
         self.bin_scratch = t.zeros((n + 1023) // 1024, dtype=t.int32, device=dev.device)
+        self.level_scratch = t.zeros(1 + 32 * ((n + 1023) // 1024), dtype=t.int32, device=dev.device)
         self.X = t.zeros((n, P.FEATURES), dtype=t.int16, device=dev.device)
         self.Z = t.zeros((n, 8), dtype=t.float32, device=dev.device)
         self.sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
@@ -76,6 +77,16 @@ class DecisionRunner:
                                            self.ev.data_ptr(), c.get("block", 32), self.sptr), "rsx_sim8_multi_raw")
             return
         order = None
+        if c["mode"] == "levels":
+            p = self.pred
+            w = (ctypes.c_float * P.LABELS)(*[float(x) for x in c.get("weights", [1.0] * P.LABELS)])
+            rsx.check(p.L.rsx_pred_features_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.X.data_ptr(),
+                                                self.sptr), "features")
+            rsx.check(p.L.rsx_pred_forward_raw(p.wb.data_ptr(), p.w.data_ptr(), self.X.data_ptr(), n, self.Z.data_ptr(), self.sptr),
+                      "forward")
+            rsx.check(p.L.rsx_pred_levels_raw(self.Z.data_ptr(), n, w, c.get("levels", 16), self.level_scratch.data_ptr(),
+                                              self.order.data_ptr(), self.sptr), "levels")
+            order = self.order.data_ptr()
         if c["mode"] == "binned":
             p = self.pred
             thr = float(np.log(c["threshold"] / (1.0 - c["threshold"])))
@@ -91,9 +102,10 @@ class DecisionRunner:
                                           c["split"], self.sptr), "rsx_sim8_lockstep_raw")
 
     def kernels_per_step(self, config: dict | None = None) -> int:
-        """This library's kernel launches per decision (features, forward, two binning passes, the decision)."""
+        """This library's kernel launches per decision (features, forward, two binning passes or three level passes,
+        the decision)."""
         c = config or self.config
-        return 5 if c["mode"] == "binned" else 1
+        return {"binned": 5, "levels": 6}.get(c["mode"], 1)
 
     # ---- states ----
     def snapshot(self):
@@ -149,6 +161,8 @@ class DecisionRunner:
             if binning and self.pred is not None:
                 for thr, labels in ((0.3, P.ALL_LABELS), (0.5, P.ALL_LABELS)):
                     out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr, "labels": labels})
+                out.append({"mode": "levels", "block": block, "grid": self.sms, "split": split, "threshold": None, "levels": 16,
+                            "weights": [1.0] * P.LABELS})
         return out
 
     def tune(self, controls_ptrs, candidates=None, repeats: int = 1):

@@ -1,6 +1,6 @@
 """Arena-count sweep of the decision step: the plain launch, the lockstep kernel and the lockstep kernel with the learned
-binning, at 4,096 ... 1,048,576 arenas of one workload, each timed on the same decisions from the same start states,
-with the three runs' words compared (all arenas, on the device).  One JSON line per size.
+binning (two bins, and sixteen cost levels), at 4,096 ... 1,048,576 arenas of one workload, each timed on the same decisions from the same start states,
+with the runs' words compared (all arenas, on the device).  One JSON line per size.
 
   python rocketsim-cuda_b200/sweep.py [--sizes 4096,16384,65536,262144,1048576] [--decisions 4] [--mix headline]
 """
@@ -49,7 +49,8 @@ def main():
         base = {"block": 448, "grid": run.sms, "split": 7}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
-                          ("binned", {"mode": "binned", "threshold": 0.5, **base})]:
+                          ("binned", {"mode": "binned", "threshold": 0.5, **base}),
+                          ("levels", {"mode": "levels", "levels": 16, "weights": [1.0] * 6, **base})]:
             run.restore(start)
             run.step(ctl[0].data_ptr(), cfg)  # the first launch of a kernel loads it: outside the timing
             run.stream.synchronize()
@@ -66,6 +67,7 @@ def main():
         print(json.dumps({"arenas": n, "mix": args.mix, "decisions": args.decisions, "train_s": round(train_s, 2), **out,
                           "lockstep_vs_plain": out["plain"]["ms_per_decision"] / out["lockstep"]["ms_per_decision"],
                           "binned_vs_plain": out["plain"]["ms_per_decision"] / out["binned"]["ms_per_decision"],
+                          "levels_vs_plain": out["plain"]["ms_per_decision"] / out["levels"]["ms_per_decision"],
                           "bit_exact_all_arenas": bool(exact)}), flush=True)
         del words, start
         run.free()

@@ -233,3 +233,32 @@ def test_training_lowers_loss_and_binning_orders_heavy_first():
     assert np.all(np.diff(o[:h]) > 0) and np.all(np.diff(o[h:]) > 0)
     m = P.recall_precision(z, Y)
     assert m["any"][0] > 0.9 and m["any"][1] > 0.9
+
+
+@pytest.mark.gpu
+def test_cost_levels_order_is_a_stable_descending_sort():
+    """rsx_pred_levels_raw on logits of +-30 (each output's probability 0 or 1 to FP32 precision, so an arena's expected
+    contact count is its number of set outputs k and, with 7 levels and the maximum 6, its level floor(7k / 6) lies far
+    from a level boundary): the order is the stable sort by level, highest first, over several blocks."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(9)
+    n = 5000
+    on = rng.random((n, 6)) < 0.3
+    on[17] = True  # one arena with all six: the batch maximum is 6
+    z = np.zeros((n, 8), np.float32)
+    z[:, :6] = np.where(on, 30.0, -30.0)
+    Z = torch.from_numpy(z).to(dev)
+    order = torch.zeros(n, dtype=torch.int32, device=dev)
+    scratch = torch.zeros(1 + 7 * ((n + 1023) // 1024), dtype=torch.int32, device=dev)
+    import rsx
+
+    L = P._bind()
+    w = (ctypes.c_float * 6)(*([1.0] * 6))
+    rsx.check(L.rsx_pred_levels_raw(Z.data_ptr(), n, w, 7, scratch.data_ptr(), order.data_ptr(), None), "levels")
+    torch.cuda.synchronize()
+    k = on.sum(1)
+    level = np.minimum(k * 7 // 6, 6)
+    want = np.argsort(-level, kind="stable")
+    assert np.array_equal(order.cpu().numpy(), want)
