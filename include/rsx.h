@@ -163,6 +163,12 @@ int rsx_pred_labels_raw(const uint32_t* d_event_or, uint32_t n, uint8_t* d_label
 /* logits[n][8] (FP32; outputs 6, 7 unused) */
 int rsx_pred_forward_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
                          void* stream);
+/* The same forward on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory; 128 arenas per
+ * tile, one CTA per SM): inference only (training keeps rsx_pred_forward_raw, which also saves activations).  Logits
+ * equal rsx_pred_forward_raw's up to FP32 summation order.  d_error[0] is set to 1 if a bounded wait for the tensor
+ * cores gave up (the logits are then incomplete); features and logits 16-byte aligned. */
+int rsx_pred_forward_tc_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
+                            uint32_t* d_error, void* stream);
 /* BF16 elements of the training scratch for a batch of n */
 uint64_t rsx_pred_scratch_elems(uint32_t n);
 /* gradients of L = (1/n) sum over the batch and the 6 outputs of the binary cross-entropy: d_grad[RSX_PRED_PARAMS]

@@ -37,6 +37,7 @@ cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* sa
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
                                  float c2, cudaStream_t s);
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
+cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, uint32_t* err, cudaStream_t s);
 cudaError_t rsx_launch_pred_levels(const float* logits, uint32_t n, const float* weights, int levels, uint32_t* scratch, uint32_t* order,
                                    cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
@@ -413,6 +414,15 @@ int rsx_pred_bin_raw(const float* d_logits, uint32_t n, float threshold_logit, u
   if (!d_logits || !d_scratch || !d_order || !d_heavy_count) return RSX_E_ARG;
   if (n == 0) return RSX_OK;
   RSX_CK(rsx_launch_pred_bin(d_logits, n, threshold_logit, label_mask, d_scratch, d_order, d_heavy_count, (cudaStream_t)stream));
+  return RSX_OK;
+}
+
+int rsx_pred_forward_tc_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
+                            uint32_t* d_error, void* stream) {
+  if (!d_w_bf16 || !d_w_f32 || !d_features || !d_logits || !d_error || ((uintptr_t)d_features & 15u) || ((uintptr_t)d_logits & 15u))
+    return rsx_set_last_error(RSX_E_ARG, "rsx_pred_forward_tc_raw: null buffer, or features / logits not 16-byte aligned");
+  if (n == 0) return RSX_OK;
+  RSX_CK(rsx_launch_pred_forward_tc(d_w_bf16, d_w_f32, d_features, n, d_logits, d_error, (cudaStream_t)stream));
   return RSX_OK;
 }
 

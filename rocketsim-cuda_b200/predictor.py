@@ -51,6 +51,7 @@ def _bind():
     L.rsx_pred_to_bf16_raw.argtypes = [vp, vp, vp]
     L.rsx_pred_bin_raw.argtypes = [vp, u32, ctypes.c_float, u32, vp, vp, vp, vp]
     L.rsx_pred_levels_raw.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32, vp, vp, vp]
+    L.rsx_pred_forward_tc_raw.argtypes = [vp, vp, vp, u32, vp, vp, vp]
     L._pred_bound = True
     return L
 
@@ -113,6 +114,17 @@ class ContactPredictor:
 
     # ---- network ----
     def logits(self, X, n: int, out=None):
+        """Inference on the tensor cores (tcgen05: rsx_pred_forward_tc_raw)."""
+        t = self.torch
+        Z = out if out is not None else t.empty((n, 8), dtype=t.float32, device=self.device)
+        if not hasattr(self, "tc_error"):
+            self.tc_error = t.zeros(1, dtype=t.int32, device=self.device)
+        rsx.check(self.L.rsx_pred_forward_tc_raw(self.wb.data_ptr(), self.w.data_ptr(), X.data_ptr(), n, Z.data_ptr(),
+                                                 self.tc_error.data_ptr(), self.stream), "rsx_pred_forward_tc_raw")
+        return Z
+
+    def logits_mma_sync(self, X, n: int, out=None):
+        """The same forward on mma.sync (the training kernels' forward)."""
         t = self.torch
         Z = out if out is not None else t.empty((n, 8), dtype=t.float32, device=self.device)
         rsx.check(self.L.rsx_pred_forward_raw(self.wb.data_ptr(), self.w.data_ptr(), X.data_ptr(), n, Z.data_ptr(), self.stream),

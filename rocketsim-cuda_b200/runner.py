@@ -82,8 +82,7 @@ class DecisionRunner:
             w = (ctypes.c_float * P.LABELS)(*[float(x) for x in c.get("weights", [1.0] * P.LABELS)])
             rsx.check(p.L.rsx_pred_features_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.X.data_ptr(),
                                                 self.sptr), "features")
-            rsx.check(p.L.rsx_pred_forward_raw(p.wb.data_ptr(), p.w.data_ptr(), self.X.data_ptr(), n, self.Z.data_ptr(), self.sptr),
-                      "forward")
+            p.logits(self.X, n, out=self.Z)
             rsx.check(p.L.rsx_pred_levels_raw(self.Z.data_ptr(), n, w, c.get("levels", 16), self.level_scratch.data_ptr(),
                                               self.order.data_ptr(), self.sptr), "levels")
             order = self.order.data_ptr()
@@ -92,8 +91,7 @@ class DecisionRunner:
             thr = float(np.log(c["threshold"] / (1.0 - c["threshold"])))
             rsx.check(p.L.rsx_pred_features_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.X.data_ptr(),
                                                 self.sptr), "features")
-            rsx.check(p.L.rsx_pred_forward_raw(p.wb.data_ptr(), p.w.data_ptr(), self.X.data_ptr(), n, self.Z.data_ptr(), self.sptr),
-                      "forward")
+            p.logits(self.X, n, out=self.Z)
             rsx.check(p.L.rsx_pred_bin_raw(self.Z.data_ptr(), n, thr, c.get("labels", P.ALL_LABELS), self.bin_scratch.data_ptr(),
                                            self.order.data_ptr(), self.heavy.data_ptr(), self.sptr), "bin")
             order = self.order.data_ptr()

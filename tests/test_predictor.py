@@ -262,3 +262,32 @@ def test_cost_levels_order_is_a_stable_descending_sort():
     level = np.minimum(k * 7 // 6, 6)
     want = np.argsort(-level, kind="stable")
     assert np.array_equal(order.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 4099, 65536])
+def test_tensor_core_forward_matches_mma_sync_forward(n):
+    """rsx_pred_forward_tc_raw (tcgen05.mma, accumulators in tensor memory) against rsx_pred_forward_raw (mma.sync)
+    on the same BF16 features and weights: the same BF16 products, FP32 sums in another order, and activations rounded
+    to BF16 between layers in both, so the logits agree to within a few BF16 steps."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(n)
+    pr = P.ContactPredictor(dev, seed=7)
+    Xf = rng.normal(0, 1, (n, 48)).astype(np.float32)
+    X = torch.from_numpy((bf16(Xf).view(np.uint32) >> 16).astype(np.uint16).view(np.int16)).to(dev)
+    ref = pr.logits_mma_sync(X, n).clone()
+    got = torch.full_like(ref, float("nan"))
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    L = P._bind()
+    rsx_mod = __import__("rsx")
+    rsx_mod.check(L.rsx_pred_forward_tc_raw(pr.wb.data_ptr(), pr.w.data_ptr(), X.data_ptr(), n, got.data_ptr(), err.data_ptr(), None),
+                  "forward_tc")
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    r, g = ref.cpu().numpy()[:, :6], got.cpu().numpy()[:, :6]
+    assert np.all(np.isfinite(g))
+    scale = float(np.abs(r).max()) + 1e-6
+    assert float(np.abs(g - r).max()) < 0.03 * scale, (float(np.abs(g - r).max()), scale)
+    assert float(np.linalg.norm(g - r) / np.linalg.norm(r)) < 5e-3
