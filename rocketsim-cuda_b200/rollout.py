@@ -63,7 +63,7 @@ class Rollout:
                 ev1.record(run.stream)
                 # labels of this decision, the predictor's guesses made before it, and training samples
                 Y = run.pred.labels(run.ev.data_ptr(), n)
-                if self.config["mode"] == "binned":
+                if self.config["mode"] in ("binned", "levels"):
                     guess = (run.Z[:, :P.LABELS] > 0.0).any(dim=1)
                     truth = Y != 0
                     tp += int((guess & truth).sum())
@@ -107,6 +107,8 @@ def main():
     ap.add_argument("--mix", default="contact", choices=["contact", "headline"])
     ap.add_argument("--pool", type=int, default=16, help="control sets cycled through")
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--order", default="levels", choices=["levels", "binned"],
+                    help="the learned order: 16 cost levels (several claim rounds) or two bins")
     args = ap.parse_args()
     import torch
 
@@ -128,11 +130,13 @@ def main():
     t0 = time.perf_counter()
     run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
     train_s = time.perf_counter() - t0
-    cfg = {"mode": "binned", "block": 448, "grid": run.sms, "split": 7, "threshold": 0.5}
+    cfg = {"mode": args.order, "block": 448, "grid": run.sms, "split": 7, "threshold": 0.5}
+    if args.order == "levels":
+        cfg.update({"levels": 16, "weights": [1.0] * 6})
     ro = Rollout(run, pool, reset_seed=args.seed * 7919, mix=mix, config=cfg)
     windows = ro.run_decisions(args.decisions, args.retrain_every)
     total_ms = sum(w["ms_per_decision"] * (w["decisions"][1] - w["decisions"][0] + 1) for w in windows)
-    print(json.dumps({"arenas": n, "decisions": args.decisions, "mix": args.mix, "retrain_every": args.retrain_every,
+    print(json.dumps({"arenas": n, "decisions": args.decisions, "mix": args.mix, "order": args.order, "retrain_every": args.retrain_every,
                       "initial_train_s": round(train_s, 2), "arena_ticks_per_s": n * 8 * args.decisions / (total_ms / 1e3),
                       "windows": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in w.items()} for w in windows]}))
 
