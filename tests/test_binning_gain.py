@@ -1,6 +1,6 @@
 """What the trained contact predictor gains: the lockstep kernel over the identity order, over an untrained network's
-order and over the trained network's order, 262,144 arenas of the headline mix (several claim rounds per SM, where the
-order matters), timed on the same decisions from the same start states.  The test checks what must hold — the three
+order and over the trained network's orders (two bins, sixteen cost levels), 262,144 arenas of the headline mix
+(several claim rounds per SM, where the order matters), timed on the same decisions from the same start states.  The test checks what must hold — the three
 give the same words, and the trained network's recall and precision on these decisions — and prints the timings (run
 with -s to see them); the speed-up itself is a measurement, not a pass condition."""
 import json
@@ -50,8 +50,9 @@ def test_trained_order_gain_is_measured_and_exact(rsx):
         run.pred = None
         run.train_predictor(control_seed=777, decisions=8)
         t_tr, w_tr, r_tr = timed({"mode": "binned", "threshold": 0.5, **base})
-        assert np.array_equal(w_id, w_un) and np.array_equal(w_id, w_tr) and np.array_equal(w_id, for_warm[1])
-        assert np.array_equal(r_id, r_un) and np.array_equal(r_id, r_tr)
+        t_lv, w_lv, r_lv = timed({"mode": "levels", "levels": 16, "weights": [1.0] * 6, **base})
+        assert np.array_equal(w_id, w_un) and np.array_equal(w_id, w_tr) and np.array_equal(w_id, for_warm[1]) and np.array_equal(w_id, w_lv)
+        assert np.array_equal(r_id, r_un) and np.array_equal(r_id, r_tr) and np.array_equal(r_id, r_lv)
         # recall / precision of the trained network on these decisions
         run.restore(start)
         Zs, Ys = [], []
@@ -64,7 +65,8 @@ def test_trained_order_gain_is_measured_and_exact(rsx):
         m = P.recall_precision(torch.cat(Zs).cpu().numpy(), torch.cat(Ys).cpu().numpy())
         assert m["any"][0] > 0.8 and m["any"][1] > 0.8, m["any"]
         print(json.dumps({"arenas": n, "decisions": D, "ms_identity_order": round(t_id, 2), "ms_untrained_order": round(t_un, 2),
-                          "ms_trained_order": round(t_tr, 2), "gain_vs_identity": round(t_id / t_tr, 4),
+                          "ms_trained_order": round(t_tr, 2), "ms_trained_levels": round(t_lv, 2), "gain_vs_identity": round(t_id / t_tr, 4),
+                          "levels_gain_vs_identity": round(t_id / t_lv, 4),
                           "gain_vs_untrained": round(t_un / t_tr, 4), "any_contact_recall_precision": [round(float(x), 3) for x in m["any"][:2]]}))
         run.free()
     finally:
