@@ -1,8 +1,9 @@
 """What the trained contact predictor gains: the lockstep kernel over the identity order, over an untrained network's
 order and over the trained network's orders (two bins, sixteen cost levels), 262,144 arenas of the headline mix
-(several claim rounds per SM, where the order matters), timed on the same decisions from the same start states.  The test checks what must hold — the three
-give the same words, and the trained network's recall and precision on these decisions — and prints the timings (run
-with -s to see them); the speed-up itself is a measurement, not a pass condition."""
+(several claim rounds per SM, where the order matters), timed on the same decisions from the same start states.  The
+test checks what must hold — every order gives the same words, and the trained network's recall and precision on
+these decisions — and prints the timings (run with -s to see them); the speed-ups are measurements, not pass
+conditions."""
 import json
 import os
 import sys
