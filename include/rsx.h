@@ -164,15 +164,16 @@ int rsx_pred_labels_raw(const uint32_t* d_event_or, uint32_t n, uint8_t* d_label
 int rsx_pred_forward_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
                          void* stream);
 /* The same forward on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor memory; 128 arenas per
- * tile, one CTA per SM): inference only (training keeps rsx_pred_forward_raw, which also saves activations).  Logits
- * equal rsx_pred_forward_raw's up to FP32 summation order.  d_error[0] is set to 1 if a bounded wait for the tensor
- * cores gave up (the logits are then incomplete); features and logits 16-byte aligned. */
+ * tile, one CTA per SM), the one inference and training use (training's forward also saves the activations).
+ * Logits equal rsx_pred_forward_raw's up to FP32 summation order.  d_error[0] is set to 1 if a bounded wait for the
+ * tensor cores gave up (the logits are then incomplete); features and logits 16-byte aligned. */
 int rsx_pred_forward_tc_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, uint32_t n, float* d_logits,
                             uint32_t* d_error, void* stream);
 /* BF16 elements of the training scratch for a batch of n */
 uint64_t rsx_pred_scratch_elems(uint32_t n);
 /* gradients of L = (1/n) sum over the batch and the 6 outputs of the binary cross-entropy: d_grad[RSX_PRED_PARAMS]
- * (overwritten), d_loss[0] = n L, d_logits[n][8] the forward's logits */
+ * (overwritten), d_loss[0] = n L, d_logits[n][8] the forward's logits.  The forward runs on tcgen05 (its wait flag in
+ * the scratch's last two elements), the backward and weight gradients on mma.sync. */
 int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, const uint8_t* d_labels,
                            uint32_t n, uint16_t* d_scratch, float* d_logits, float* d_grad, float* d_loss, void* stream);
 /* one Adam step (beta 0.9, 0.999, eps 1e-8) of the FP32 master weights with moments d_m, d_v; refreshes the BF16 copy */

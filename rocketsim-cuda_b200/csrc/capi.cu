@@ -37,7 +37,8 @@ cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* sa
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
                                  float c2, cudaStream_t s);
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
-cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, uint32_t* err, cudaStream_t s);
+cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, uint32_t* err,
+                                       cudaStream_t s);
 cudaError_t rsx_launch_pred_levels(const float* logits, uint32_t n, const float* weights, int levels, uint32_t* scratch, uint32_t* order,
                                    cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
@@ -351,7 +352,7 @@ int rsx_l2_persist_raw(const void* d_ptr, uint64_t bytes, float hit_ratio, void*
 }
 
 // ---- the contact predictor ----
-uint64_t rsx_pred_scratch_elems(uint32_t n) { return 2ull * (3ull * n + 16) * 128 + (uint64_t)(n + 16) * 8; }
+uint64_t rsx_pred_scratch_elems(uint32_t n) { return 2ull * (3ull * n + 16) * 128 + (uint64_t)(n + 16) * 8 + 2; }
 
 int rsx_pred_features_raw(const uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
                           uint16_t* d_features, void* stream) {
@@ -385,7 +386,8 @@ int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const
   RSX_CK(cudaMemsetAsync(d_grad, 0, RSX_PRED_PARAMS * sizeof(float), s));
   RSX_CK(cudaMemsetAsync(d_loss, 0, sizeof(float), s));
   RSX_CK(cudaMemsetAsync(save + 3ull * n * 128, 0, 16 * 128 * 2, s));  // the rows past n that the last tile reads
-  RSX_CK(rsx_launch_pred_forward(d_w_bf16, d_w_f32, d_features, n, d_logits, save, s));
+  uint32_t* tc_error = reinterpret_cast<uint32_t*>(dz + (uint64_t)(n + 16) * 8);  // the scratch's last two elements
+  RSX_CK(rsx_launch_pred_forward_tc(d_w_bf16, d_w_f32, d_features, n, d_logits, save, tc_error, s));
   RSX_CK(rsx_launch_pred_backward(d_w_bf16, d_w_f32, d_logits, d_labels, save, n, 1.0f / (float)n, dz, dsave, d_loss, s));
   RSX_CK(rsx_launch_pred_wgrads(d_features, dz, save, dsave, n, d_grad, s));
   return RSX_OK;
@@ -422,7 +424,7 @@ int rsx_pred_forward_tc_raw(const uint16_t* d_w_bf16, const float* d_w_f32, cons
   if (!d_w_bf16 || !d_w_f32 || !d_features || !d_logits || !d_error || ((uintptr_t)d_features & 15u) || ((uintptr_t)d_logits & 15u))
     return rsx_set_last_error(RSX_E_ARG, "rsx_pred_forward_tc_raw: null buffer, or features / logits not 16-byte aligned");
   if (n == 0) return RSX_OK;
-  RSX_CK(rsx_launch_pred_forward_tc(d_w_bf16, d_w_f32, d_features, n, d_logits, d_error, (cudaStream_t)stream));
+  RSX_CK(rsx_launch_pred_forward_tc(d_w_bf16, d_w_f32, d_features, n, d_logits, nullptr, d_error, (cudaStream_t)stream));
   return RSX_OK;
 }
 

@@ -1,8 +1,8 @@
 // The contact predictor's inference on the 5th-generation tensor cores: the 48 -> 128 -> 128 -> 128 -> 6 MLP forward
 // for tiles of 128 arenas with tcgen05.mma (BF16 operands from shared memory, FP32 accumulators in tensor memory),
 // the epilogues (bias, ReLU, BF16) read back with tcgen05.ld.  Same parameters and outputs as k_pred_forward (the
-// mma.sync version, which training keeps because it also saves the activations for the backward pass); the logits
-// agree to FP32 rounding of the same BF16 products.
+// mma.sync version), including the saved activations that training's backward pass reads; the logits agree to FP32
+// rounding of the same BF16 products.
 //
 // Per CTA (128 threads, one per accumulator row / TMEM lane): the four weight matrices are staged once in shared
 // memory in the UMMA canonical K-major layout without swizzle (8 x 16-byte core matrices: element (r, k) at
@@ -94,7 +94,7 @@ __device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.prox
 
 extern "C" __global__ void __launch_bounds__(kRows, 1) k_pred_forward_tc(const __nv_bfloat16* __restrict__ wb, const float* __restrict__ wf,
                                                                          const __nv_bfloat16* __restrict__ X, uint32_t n, float* __restrict__ logits,
-                                                                         uint32_t* err) {
+                                                                         __nv_bfloat16* __restrict__ save, uint32_t* err) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
@@ -199,6 +199,11 @@ extern "C" __global__ void __launch_bounds__(kRows, 1) k_pred_forward_tc(const _
           }
           *reinterpret_cast<uint4*>(sm + kAct + canon(tid, c0, kHid)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
           *reinterpret_cast<uint4*>(sm + kAct + canon(tid, c0 + 8, kHid)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          if (save && live) {  // the activations for the backward pass: [layer][n][128] BF16, row-major
+            uint4* dst = reinterpret_cast<uint4*>(save + ((size_t)layer * n + row) * kHid + c0);
+            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          }
         }
       } else {
         float v[16];
@@ -222,7 +227,8 @@ extern "C" __global__ void __launch_bounds__(kRows, 1) k_pred_forward_tc(const _
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
-cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, uint32_t* err, cudaStream_t s) {
+cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, uint32_t* err,
+                                       cudaStream_t s) {
   static int configured[64];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -236,6 +242,6 @@ cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const vo
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint32_t tiles = (n + kRows - 1) / kRows;
   const uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
-  k_pred_forward_tc<<<grid, kRows, kSmemBytes, s>>>((const __nv_bfloat16*)wb, wf, (const __nv_bfloat16*)X, n, logits, err);
+  k_pred_forward_tc<<<grid, kRows, kSmemBytes, s>>>((const __nv_bfloat16*)wb, wf, (const __nv_bfloat16*)X, n, logits, (__nv_bfloat16*)save, err);
   return cudaGetLastError();
 }
