@@ -40,6 +40,10 @@ TRAFFIC_PER_ARENA_DECISION = 4.716e9 / 32768
 # rewards written
 OBS_BYTES_PER_ARENA = 103 * 4 + 9 + 2 * 208 + 2 * 4
 OBS_REPS = 20
+# instruction counts of the lockstep kernel (block 448, split 7) from the same ncu capture as the traffic: 740.69 M warp
+# instructions with 7.79 of 32 lanes active on average for one 32,768-arena decision (8 ticks)
+WARP_INST_PER_ARENA_TICK = 740.69e6 / (32768 * 8)
+LANES_ACTIVE = 7.79
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
 
@@ -375,6 +379,19 @@ def run_ours(args):
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": mean_ms}
 
+    # the second roofline: instruction issue (4 schedulers per SM issue one warp instruction per cycle each)
+    sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
+    clk_hz = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    warp_issue_peak = sms * 4 * clk_hz
+    per_gpu = value / world_size
+    roofline_issue = {"bound": "issue", "unit": "warp instructions/s",
+                      "achieved": WARP_INST_PER_ARENA_TICK * per_gpu, "peak": warp_issue_peak,
+                      "frac": WARP_INST_PER_ARENA_TICK * per_gpu / warp_issue_peak,
+                      "simt_efficiency": LANES_ACTIVE / 32.0,
+                      "thread_instruction_frac": WARP_INST_PER_ARENA_TICK * LANES_ACTIVE * per_gpu / (warp_issue_peak * 32),
+                      "per_arena_tick": {"warp_instructions": WARP_INST_PER_ARENA_TICK, "lanes_active": LANES_ACTIVE},
+                      "source": "ncu capture of k_sim8_lockstep_t448<7> at 32,768 arenas (instructions per arena-tick), sm_max_mhz"} \
+        if config["mode"] != "plain" else None
     observe = {"kernel": "k_observe", "ms_per_launch": obs_ms, "arenas": n,
                "achieved_gbs": OBS_BYTES_PER_ARENA * n / (obs_ms / 1e3) / 1e9,
                "frac": OBS_BYTES_PER_ARENA * n / (obs_ms / 1e3) / 1e9 / peak, "bytes_per_arena": OBS_BYTES_PER_ARENA,
@@ -410,6 +427,7 @@ def run_ours(args):
             "predictor": pred_info,
             "e2e": {"value": e2e, "unit": "arena-ticks/s", "h2d_bytes_per_step": n * 64, "d2h_bytes_per_step": n * 4},
             "roofline": roofline,
+            "roofline_issue": roofline_issue,
             "observe": observe,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
