@@ -16,15 +16,17 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/rsx.h"
+#include "tcgen05.cuh"
+
+using namespace rsx::tc;
 
 namespace {
 
-constexpr int kIn = RSX_PRED_FEATURES, kInPad = 64, kHid = 128, kOutPad = 8, kOutMma = 16;
+constexpr int kIn = RSX_PRED_FEATURES, kInPad = 64, kHid = 128, kOutPad = 8, kOutMma = 16, kOut = RSX_PRED_LABELS;
 constexpr int oW1 = 0, ob1 = oW1 + kHid * kIn, oW2 = ob1 + kHid, ob2 = oW2 + kHid * kHid, oW3 = ob2 + kHid, ob3 = oW3 + kHid * kHid,
               oW4 = ob3 + kHid, ob4 = oW4 + kOutPad * kHid;
 constexpr int kRows = 128;             // arenas per tile = MMA M = threads per CTA = TMEM lanes
 constexpr uint32_t kTmemCols = 128;    // one FP32 accumulator of N <= 128
-constexpr long long kWaitCycles = 1ll << 28;
 
 // shared memory (bytes; every operand tile 1024-aligned)
 constexpr uint32_t kW1 = 0, kW1Bytes = kHid * kInPad * 2;
@@ -35,60 +37,6 @@ constexpr uint32_t kAct = kW4 + kW4Bytes, kActBytes = kRows * kHid * 2;
 constexpr uint32_t kBias = kAct + kActBytes, kBiasBytes = (3 * kHid + kOutMma) * 4;
 constexpr uint32_t kMisc = kBias + kBiasBytes;  // mbarrier (8 bytes), TMEM address (4 bytes)
 constexpr uint32_t kSmemBytes = kMisc + 16 + 1024;  // + alignment slack
-
-// byte offset of element (r, k) of a K-major operand with K columns in the canonical no-swizzle layout
-__device__ __forceinline__ uint32_t canon(uint32_t r, uint32_t k, uint32_t K) {
-  return (r >> 3) * (K / 8 * 128) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
-}
-
-// shared-memory matrix descriptor (SM100 UMMA): start >> 4 in bits 0-13, leading-dimension byte offset (the K
-// direction between 8-element core matrices) >> 4 in bits 16-29, stride byte offset (between 8-row groups) >> 4 in
-// bits 32-45, version 1 in bits 46-47, no swizzle (layout type 0 in bits 61-63)
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
-         (1ull << 46);
-}
-// instruction descriptor, kind::f16: FP32 accumulate (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
-// N >> 3 in bits 17-22, M >> 4 in bits 24-28
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t M, uint32_t N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d), "l"(a),
-      "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  const long long t0 = clock64();
-  for (;;) {
-    uint32_t done;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(done)
-                 : "r"(mbar), "r"(parity)
-                 : "memory");
-    if (done) return true;
-    if (clock64() - t0 > kWaitCycles) return false;
-  }
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
-        "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 }  // namespace
 
@@ -225,6 +173,172 @@ extern "C" __global__ void __launch_bounds__(kRows, 1) k_pred_forward_tc(const _
   __syncthreads();
   fence_after();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// ---- backward through the layers on tcgen05: dZ = (sigmoid(z) - y) / n on the six outputs, then dH3 = (dZ . W4)
+// masked by H3 > 0, dH2 = (dH3 . W3) masked by H2 > 0, dH1 = (dH2 . W2) masked by H1 > 0 (BF16; [n][8] and
+// [3][n][128], the layout the weight-gradient kernels read), and the loss sum.  The weights are staged transposed
+// (B operand element (i, o) = W[o][i], K-major), the dZ / dH tiles are the A operands. ----
+namespace {
+constexpr uint32_t bW4T = 0, bW4TBytes = kHid * 16 * 2;                 // N = 128 x K = 16 (outputs 8..15 zero)
+constexpr uint32_t bW3T = bW4T + bW4TBytes, bW3TBytes = kHid * kHid * 2;
+constexpr uint32_t bW2T = bW3T + bW3TBytes;
+constexpr uint32_t bAct = bW2T + bW3TBytes;
+constexpr uint32_t bMisc = bAct + kActBytes;
+constexpr uint32_t kBwdSmemBytes = bMisc + 16 + 1024;
+}  // namespace
+
+extern "C" __global__ void __launch_bounds__(kRows, 1) k_pred_backward_tc(const __nv_bfloat16* __restrict__ wb, const float* __restrict__ logits,
+                                                                          const uint8_t* __restrict__ Y, const __nv_bfloat16* __restrict__ save,
+                                                                          uint32_t n, float inv_scale, __nv_bfloat16* __restrict__ dz,
+                                                                          __nv_bfloat16* __restrict__ dsave, float* loss_sum, uint32_t* err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + bMisc + 8);
+  const uint32_t mbar = sbase + bMisc;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  for (uint32_t i = tid; i < (uint32_t)(kHid * 16); i += kRows) {  // element (i, o) of W4^T
+    uint32_t r = i / 16, o = i % 16;
+    *reinterpret_cast<__nv_bfloat16*>(sm + bW4T + canon(r, o, 16)) = o < (uint32_t)kOutPad ? wb[oW4 + o * kHid + r] : zero;
+  }
+  for (uint32_t i = tid; i < (uint32_t)(kHid * kHid); i += kRows) {  // W[o][i] -> element (i, o)
+    uint32_t o = i / kHid, r = i % kHid;
+    *reinterpret_cast<__nv_bfloat16*>(sm + bW3T + canon(r, o, kHid)) = wb[oW3 + i];
+    *reinterpret_cast<__nv_bfloat16*>(sm + bW2T + canon(r, o, kHid)) = wb[oW2 + i];
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + bMisc + 8), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = (warp * 32u) << 16;
+  uint32_t phase = 0;
+  bool ok = true;
+  float loss = 0.0f;
+
+  const uint32_t tiles = (n + kRows - 1) / kRows;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint32_t row = tile * kRows + tid;
+    const bool live = row < n;
+    // dZ (K = 16: outputs 0..5, zero elsewhere) into the A tile and, for outputs 0..7, into dz
+    uint32_t pk[8];
+#pragma unroll
+    for (int o2 = 0; o2 < 8; ++o2) {
+      float d2[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int o = 2 * o2 + h;
+        float d = 0.0f;
+        if (live && o < kOut) {
+          const float zz = logits[(size_t)row * kOutPad + o];
+          const float y = (Y[row] >> o) & 1u ? 1.0f : 0.0f;
+          const float p = 1.0f / (1.0f + expf(-zz));
+          d = (p - y) * inv_scale;
+          loss += fmaxf(zz, 0.0f) - zz * y + log1pf(expf(-fabsf(zz)));
+        }
+        d2[h] = d;
+      }
+      __nv_bfloat162 hv = __floats2bfloat162_rn(d2[0], d2[1]);
+      pk[o2] = *reinterpret_cast<uint32_t*>(&hv);
+    }
+    *reinterpret_cast<uint4*>(sm + bAct + canon(tid, 0, 16)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(sm + bAct + canon(tid, 8, 16)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    if (live) *reinterpret_cast<uint4*>(dz + (size_t)row * kOutPad) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    // three layers down: (operand K, transposed weights, saved activation layer = mask, gradient layer)
+#pragma unroll 1
+    for (int step = 0; step < 3 && ok; ++step) {
+      const uint32_t K = step == 0 ? 16u : (uint32_t)kHid;
+      const uint32_t wofs = step == 0 ? bW4T : step == 1 ? bW3T : bW2T;
+      const int layer = 2 - step;  // H3, H2, H1 and dH3, dH2, dH1
+      fence_smem_to_async();
+      fence_before();
+      __syncthreads();
+      fence_after();
+      if (tid == 0) {
+        const uint32_t sbo = K / 8 * 128;
+#pragma unroll 1
+        for (uint32_t s = 0; s < K / 16; ++s)
+          mma_bf16(tmem, smem_desc(sbase + bAct + s * 256, 128, sbo), smem_desc(sbase + wofs + s * 256, 128, sbo), instr_desc(kRows, kHid),
+                   s > 0 ? 1u : 0u);
+        mma_commit(mbar);
+      }
+      __syncwarp();
+      if (!__syncthreads_and(mbar_wait(mbar, phase) ? 1 : 0)) {
+        ok = false;
+        break;
+      }
+      phase ^= 1u;
+      fence_after();
+      const __nv_bfloat16* hrow = save + ((size_t)layer * n + row) * kHid;
+      __nv_bfloat16* grow = dsave + ((size_t)layer * n + row) * kHid;
+#pragma unroll 1
+      for (uint32_t c0 = 0; c0 < (uint32_t)kHid; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + lane_base + c0, v);
+        uint4 hm[2] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u)};
+        if (live) {
+          hm[0] = reinterpret_cast<const uint4*>(hrow + c0)[0];
+          hm[1] = reinterpret_cast<const uint4*>(hrow + c0)[1];
+        }
+        const __nv_bfloat16* hb = reinterpret_cast<const __nv_bfloat16*>(hm);
+        uint32_t q[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float lo = __bfloat162float(hb[2 * i]) > 0.0f ? v[2 * i] : 0.0f;
+          const float hi = __bfloat162float(hb[2 * i + 1]) > 0.0f ? v[2 * i + 1] : 0.0f;
+          __nv_bfloat162 h2v = __floats2bfloat162_rn(lo, hi);
+          q[i] = *reinterpret_cast<uint32_t*>(&h2v);
+        }
+        if (step < 2) {
+          *reinterpret_cast<uint4*>(sm + bAct + canon(tid, c0, kHid)) = make_uint4(q[0], q[1], q[2], q[3]);
+          *reinterpret_cast<uint4*>(sm + bAct + canon(tid, c0 + 8, kHid)) = make_uint4(q[4], q[5], q[6], q[7]);
+        }
+        if (live) {
+          reinterpret_cast<uint4*>(grow + c0)[0] = make_uint4(q[0], q[1], q[2], q[3]);
+          reinterpret_cast<uint4*>(grow + c0)[1] = make_uint4(q[4], q[5], q[6], q[7]);
+        }
+      }
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1u);
+    mbar_wait(mbar, phase);
+  }
+  for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+  if ((tid & 31) == 0 && loss_sum) atomicAdd(loss_sum, loss);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+cudaError_t rsx_launch_pred_backward_tc(const void* wb, const float* logits, const uint8_t* Y, const void* save, uint32_t n, float inv_scale,
+                                        void* dz, void* dsave, float* loss_sum, uint32_t* err, cudaStream_t s) {
+  static int configured[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !configured[dev]) {
+    e = cudaFuncSetAttribute((const void*)k_pred_backward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) configured[dev] = 1;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint32_t tiles = (n + kRows - 1) / kRows;
+  const uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+  k_pred_backward_tc<<<grid, kRows, kBwdSmemBytes, s>>>((const __nv_bfloat16*)wb, logits, Y, (const __nv_bfloat16*)save, n, inv_scale,
+                                                        (__nv_bfloat16*)dz, (__nv_bfloat16*)dsave, loss_sum, err);
+  return cudaGetLastError();
 }
 
 cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, uint32_t* err,
