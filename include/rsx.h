@@ -172,8 +172,8 @@ int rsx_pred_forward_tc_raw(const uint16_t* d_w_bf16, const float* d_w_f32, cons
 /* BF16 elements of the training scratch for a batch of n */
 uint64_t rsx_pred_scratch_elems(uint32_t n);
 /* gradients of L = (1/n) sum over the batch and the 6 outputs of the binary cross-entropy: d_grad[RSX_PRED_PARAMS]
- * (overwritten), d_loss[0] = n L, d_logits[n][8] the forward's logits.  The forward and the backward through the layers
- * run on tcgen05 (their wait flag in the scratch's last two elements), the weight gradients on mma.sync. */
+ * (overwritten), d_loss[0] = n L, d_logits[n][8] the forward's logits.  Forward, backward through the layers and the
+ * weight gradients all run on tcgen05 (their wait flag in the scratch's last two elements). */
 int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const uint16_t* d_features, const uint8_t* d_labels,
                            uint32_t n, uint16_t* d_scratch, float* d_logits, float* d_grad, float* d_loss, void* stream);
 /* one Adam step (beta 0.9, 0.999, eps 1e-8) of the FP32 master weights with moments d_m, d_v; refreshes the BF16 copy */

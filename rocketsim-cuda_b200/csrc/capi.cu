@@ -31,9 +31,6 @@ cudaError_t rsx_launch_pred_features(const uint32_t* states, const void* sds, co
                                      void* X, cudaStream_t s);
 cudaError_t rsx_launch_pred_labels(const uint32_t* ev, uint32_t n, uint8_t* Y, cudaStream_t s);
 cudaError_t rsx_launch_pred_forward(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, cudaStream_t s);
-cudaError_t rsx_launch_pred_backward(const void* wb, const float* wf, const float* logits, const uint8_t* Y, const void* save, uint32_t n,
-                                     float inv_scale, void* dz, void* dsave, float* loss_sum, cudaStream_t s);
-cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* save, const void* dsave, uint32_t n, float* grad, cudaStream_t s);
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,
                                  float c2, cudaStream_t s);
 cudaError_t rsx_launch_pred_to_bf16(const float* w, void* wb, cudaStream_t s);
@@ -41,6 +38,8 @@ cudaError_t rsx_launch_pred_forward_tc(const void* wb, const float* wf, const vo
                                        cudaStream_t s);
 cudaError_t rsx_launch_pred_backward_tc(const void* wb, const float* logits, const uint8_t* Y, const void* save, uint32_t n, float inv_scale,
                                         void* dz, void* dsave, float* loss_sum, uint32_t* err, cudaStream_t s);
+cudaError_t rsx_launch_pred_wgrads_tc(const void* X, const void* dz, const void* save, const void* dsave, uint32_t n, float* grad, uint32_t* err,
+                                      cudaStream_t s);
 cudaError_t rsx_launch_pred_levels(const float* logits, uint32_t n, const float* weights, int levels, uint32_t* scratch, uint32_t* order,
                                    cudaStream_t s);
 cudaError_t rsx_launch_pred_bin(const float* logits, uint32_t n, float thr, uint32_t mask, uint32_t* block_scratch, uint32_t* order,
@@ -391,7 +390,7 @@ int rsx_pred_gradients_raw(const uint16_t* d_w_bf16, const float* d_w_f32, const
   uint32_t* tc_error = reinterpret_cast<uint32_t*>(dz + (uint64_t)(n + 16) * 8);  // the scratch's last two elements
   RSX_CK(rsx_launch_pred_forward_tc(d_w_bf16, d_w_f32, d_features, n, d_logits, save, tc_error, s));
   RSX_CK(rsx_launch_pred_backward_tc(d_w_bf16, d_logits, d_labels, save, n, 1.0f / (float)n, dz, dsave, d_loss, tc_error, s));
-  RSX_CK(rsx_launch_pred_wgrads(d_features, dz, save, dsave, n, d_grad, s));
+  RSX_CK(rsx_launch_pred_wgrads_tc(d_features, dz, save, dsave, n, d_grad, tc_error, s));
   return RSX_OK;
 }
 

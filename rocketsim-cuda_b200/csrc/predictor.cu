@@ -1,7 +1,7 @@
 // The contact predictor: per-arena features, a 48 -> 128 -> 128 -> 128 -> 6 ReLU MLP with sigmoid outputs (BF16
-// weights and activations, FP32 accumulation on the tensor cores through mma.sync m16n8k16), its training (forward
-// with saved activations, backward, Adam on FP32 master weights), and the binning of arenas into contact-heavy and
-// quiet queues for the persistent decision kernels.
+// weights and activations, FP32 accumulation), Adam on the FP32 master weights, and the orders of arenas (two bins,
+// cost levels) for the persistent decision kernels.  The MLP's products run on tcgen05 (predictor_tc.cu: forward,
+// backward, weight gradients); the forward here, on mma.sync m16n8k16, is kept as the check of that one.
 //
 // It only schedules work: the decision kernels give the same words whatever order they take arenas in, so a wrong
 // prediction costs time, never correctness.  The six labels are the decision's event OR (the decision kernels'
@@ -219,130 +219,6 @@ extern "C" __global__ void __launch_bounds__(kWarps * 32) k_pred_forward(const _
   }
 }
 
-// ---- backward through the layers (per row): dZ, dH3, dH2, dH1 (BF16, [n][8] and [3][n][128]) and the loss sum ----
-// dZ = (sigmoid(z) - y) / scale on the 6 outputs; dHk = (dH(k+1) . W(k+1)) masked by Hk > 0.
-template <int KO, int SO>
-__device__ void layer_bwd(const __nv_bfloat16* dout, const __nv_bfloat16* w, int sw_, const __nv_bfloat16* h, __nv_bfloat16* din,
-                          __nv_bfloat16* gsave, int rows_left) {
-  // din(16 x 128) = dout(16 x KO) . W(KO x 128), W[o][i] in shared memory (row stride sw_)
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  uint32_t a[(KO + 15) / 16][4];
-#pragma unroll
-  for (int ks = 0; ks < (KO + 15) / 16; ++ks) {
-    const int k0 = ks * 16 + 2 * t;
-    a[ks][0] = ld32(dout + g * SO + k0);
-    a[ks][1] = ld32(dout + (g + 8) * SO + k0);
-    a[ks][2] = ld32(dout + g * SO + k0 + 8);
-    a[ks][3] = ld32(dout + (g + 8) * SO + k0 + 8);
-  }
-  const __nv_bfloat16 z = __float2bfloat16_rn(0.0f);
-#pragma unroll 1
-  for (int nt = 0; nt < kHid / 8; ++nt) {
-    const int n0 = nt * 8;
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int ks = 0; ks < (KO + 15) / 16; ++ks) {
-      const int k0 = ks * 16 + 2 * t;
-      auto W = [&](int o) { return o < KO ? w[o * sw_ + n0 + g] : z; };
-      uint32_t b[2] = {pack2(W(k0), W(k0 + 1)), pack2(W(k0 + 8), W(k0 + 9))};
-      mma16816(c, a[ks], b);
-    }
-    const int col = n0 + 2 * t;
-    float m0 = __bfloat162float(h[g * kHid + col]) > 0.0f ? 1.0f : 0.0f;
-    float m1 = __bfloat162float(h[g * kHid + col + 1]) > 0.0f ? 1.0f : 0.0f;
-    float m2 = __bfloat162float(h[(g + 8) * kHid + col]) > 0.0f ? 1.0f : 0.0f;
-    float m3 = __bfloat162float(h[(g + 8) * kHid + col + 1]) > 0.0f ? 1.0f : 0.0f;
-    uint32_t lo = pack2(__float2bfloat16_rn(c[0] * m0), __float2bfloat16_rn(c[1] * m1));
-    uint32_t hi = pack2(__float2bfloat16_rn(c[2] * m2), __float2bfloat16_rn(c[3] * m3));
-    *reinterpret_cast<uint32_t*>(din + g * sHid + col) = lo;
-    *reinterpret_cast<uint32_t*>(din + (g + 8) * sHid + col) = hi;
-    if (g < rows_left) *reinterpret_cast<uint32_t*>(gsave + g * kHid + col) = lo;
-    if (g + 8 < rows_left) *reinterpret_cast<uint32_t*>(gsave + (g + 8) * kHid + col) = hi;
-  }
-  __syncwarp();
-}
-
-extern "C" __global__ void __launch_bounds__(kWarps * 32) k_pred_backward(const __nv_bfloat16* wb, const float* wf, const float* logits,
-                                                                         const uint8_t* Y, const __nv_bfloat16* save, uint32_t n,
-                                                                         float inv_scale, __nv_bfloat16* dz, __nv_bfloat16* dsave,
-                                                                         float* loss_sum) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
-  load_weights(sm, wb, wf);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __nv_bfloat16* A = sm.act[warp][0];
-  __nv_bfloat16* B = sm.act[warp][1];
-  const uint32_t tiles = (n + 15) / 16;
-  float loss = 0.0f;
-  for (uint32_t tile = blockIdx.x * kWarps + warp; tile < tiles; tile += gridDim.x * kWarps) {
-    const uint32_t r0 = tile * 16;
-    const int rows = (int)min(16u, n - r0);
-    // dZ (16 x 16: outputs 0..5, zero elsewhere) into A
-    for (int i = lane; i < 16 * 16; i += 32) {
-      int r = i / 16, o = i % 16;
-      float d = 0.0f;
-      if (r < rows && o < kOut) {
-        float zz = logits[(size_t)(r0 + r) * kOutPad + o];
-        float y = (Y[r0 + r] >> o) & 1u ? 1.0f : 0.0f;
-        float p = 1.0f / (1.0f + expf(-zz));
-        d = (p - y) * inv_scale;
-        loss += fmaxf(zz, 0.0f) - zz * y + log1pf(expf(-fabsf(zz)));
-      }
-      __nv_bfloat16 bd = __float2bfloat16_rn(d);
-      A[r * sHid + o] = bd;
-      if (r < rows && o < kOutPad) dz[(size_t)(r0 + r) * kOutPad + o] = bd;
-    }
-    __syncwarp();
-    const __nv_bfloat16* h1 = save + (size_t)r0 * kHid;
-    const __nv_bfloat16* h2 = save + (size_t)n * kHid + (size_t)r0 * kHid;
-    const __nv_bfloat16* h3 = save + (size_t)2 * n * kHid + (size_t)r0 * kHid;
-    __nv_bfloat16* g1 = dsave + (size_t)r0 * kHid;
-    __nv_bfloat16* g2 = dsave + (size_t)n * kHid + (size_t)r0 * kHid;
-    __nv_bfloat16* g3 = dsave + (size_t)2 * n * kHid + (size_t)r0 * kHid;
-    // rows past n read zero activations (the save buffers are padded to whole tiles by the caller)
-    layer_bwd<kOutPad, sHid>(A, sm.w4, sHid, h3, B, g3, rows);
-    layer_bwd<kHid, sHid>(B, sm.w3, sHid, h2, A, g2, rows);
-    layer_bwd<kHid, sHid>(A, sm.w2, sHid, h1, B, g1, rows);
-  }
-  for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
-  if (lane == 0 && loss_sum) atomicAdd(loss_sum, loss);
-}
-
-// ---- weight gradients: dW[o][i] += sum_b G[b][o] A[b][i], db[o] += sum_b G[b][o] over a slice of the batch ----
-// one warp per (16-row o tile, 8-column i tile, batch slice); G is [n][go] BF16, A is [n][ai] BF16
-extern "C" __global__ void k_pred_wgrad(const __nv_bfloat16* G, int go, int no, const __nv_bfloat16* Act, int ai, int ni, uint32_t n,
-                                        uint32_t slice, float* dW, float* db) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int ot = blockIdx.x / (ni / 8), it = blockIdx.x % (ni / 8);
-  const int o0 = ot * 16, i0 = it * 8;
-  const uint32_t b_lo = blockIdx.y * slice, b_hi = min(n, b_lo + slice);
-  const __nv_bfloat16 z = __float2bfloat16_rn(0.0f);
-  auto Gv = [&](uint32_t b, int o) { return (b < b_hi && o < no) ? G[(size_t)b * go + o] : z; };
-  auto Av = [&](uint32_t b, int i) { return b < b_hi ? Act[(size_t)b * ai + i] : z; };
-  float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  for (uint32_t b0 = b_lo; b0 < b_hi; b0 += 16) {
-    const uint32_t k0 = b0 + 2 * t;
-    uint32_t a[4] = {pack2(Gv(k0, o0 + g), Gv(k0 + 1, o0 + g)), pack2(Gv(k0, o0 + g + 8), Gv(k0 + 1, o0 + g + 8)),
-                     pack2(Gv(k0 + 8, o0 + g), Gv(k0 + 9, o0 + g)), pack2(Gv(k0 + 8, o0 + g + 8), Gv(k0 + 9, o0 + g + 8))};
-    uint32_t bb[2] = {pack2(Av(k0, i0 + g), Av(k0 + 1, i0 + g)), pack2(Av(k0 + 8, i0 + g), Av(k0 + 9, i0 + g))};
-    mma16816(c, a, bb);
-  }
-  const int col = i0 + 2 * t;
-  if (o0 + g < no) {
-    atomicAdd(&dW[(o0 + g) * ni + col], c[0]);
-    atomicAdd(&dW[(o0 + g) * ni + col + 1], c[1]);
-  }
-  if (o0 + g + 8 < no) {
-    atomicAdd(&dW[(o0 + g + 8) * ni + col], c[2]);
-    atomicAdd(&dW[(o0 + g + 8) * ni + col + 1], c[3]);
-  }
-  if (it == 0 && lane < 16 && o0 + lane < no) {
-    float s = 0.0f;
-    for (uint32_t b = b_lo; b < b_hi; ++b) s += __bfloat162float(G[(size_t)b * go + o0 + lane]);
-    atomicAdd(&db[o0 + lane], s);
-  }
-}
-
 // ---- Adam on the FP32 master weights, BF16 copy refreshed ----
 extern "C" __global__ void k_pred_adam(float* w, __nv_bfloat16* wb, float* m, float* v, const float* grad, uint32_t count, float lr, float b1,
                                        float b2, float eps, float c1, float c2) {
@@ -507,14 +383,13 @@ cudaError_t rsx_launch_pred_labels(const uint32_t* ev, uint32_t n, uint8_t* Y, c
 // the shared-memory opt-in of the forward / backward kernels, once per process and device (kept out of the launch path,
 // so that launches can be captured into CUDA graphs)
 static cudaError_t set_smem(const void* fn) {
-  static int done[2][64];
+  static int done[64];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  int which = fn == (const void*)k_pred_forward ? 0 : 1;
-  if (dev >= 0 && dev < 64 && done[which][dev]) return cudaSuccess;
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pred_smem());
-  if (e == cudaSuccess && dev >= 0 && dev < 64) done[which][dev] = 1;
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = 1;
   return e;
 }
 cudaError_t rsx_launch_pred_forward(const void* wb, const float* wf, const void* X, uint32_t n, float* logits, void* save, cudaStream_t s) {
@@ -522,30 +397,6 @@ cudaError_t rsx_launch_pred_forward(const void* wb, const float* wf, const void*
   if (e != cudaSuccess) return e;
   uint32_t tiles = (n + 15) / 16, grid = min((tiles + kWarps - 1) / kWarps, 148u * 4u);
   k_pred_forward<<<grid, kWarps * 32, pred_smem(), s>>>((const __nv_bfloat16*)wb, wf, (const __nv_bfloat16*)X, n, logits, (__nv_bfloat16*)save);
-  return cudaGetLastError();
-}
-cudaError_t rsx_launch_pred_backward(const void* wb, const float* wf, const float* logits, const uint8_t* Y, const void* save, uint32_t n,
-                                     float inv_scale, void* dz, void* dsave, float* loss_sum, cudaStream_t s) {
-  cudaError_t e = set_smem((const void*)k_pred_backward);
-  if (e != cudaSuccess) return e;
-  uint32_t tiles = (n + 15) / 16, grid = min((tiles + kWarps - 1) / kWarps, 148u * 4u);
-  k_pred_backward<<<grid, kWarps * 32, pred_smem(), s>>>((const __nv_bfloat16*)wb, wf, logits, Y, (const __nv_bfloat16*)save, n, inv_scale,
-                                                        (__nv_bfloat16*)dz, (__nv_bfloat16*)dsave, loss_sum);
-  return cudaGetLastError();
-}
-cudaError_t rsx_launch_pred_wgrads(const void* X, const void* dz, const void* save, const void* dsave, uint32_t n, float* grad, cudaStream_t s) {
-  const __nv_bfloat16* x = (const __nv_bfloat16*)X;
-  const __nv_bfloat16* h = (const __nv_bfloat16*)save;
-  const __nv_bfloat16* d = (const __nv_bfloat16*)dsave;
-  const uint32_t slice = 512, ys = (n + slice - 1) / slice;
-  // layer 4: G = dZ [n][8] (6 live rows of W4), A = H3
-  k_pred_wgrad<<<dim3(1 * (kHid / 8), ys), 32, 0, s>>>((const __nv_bfloat16*)dz, kOutPad, kOut, h + (size_t)2 * n * kHid, kHid, kHid, n, slice,
-                                                      grad + oW4, grad + ob4);
-  k_pred_wgrad<<<dim3((kHid / 16) * (kHid / 8), ys), 32, 0, s>>>(d + (size_t)2 * n * kHid, kHid, kHid, h + (size_t)n * kHid, kHid, kHid, n,
-                                                                 slice, grad + oW3, grad + ob3);
-  k_pred_wgrad<<<dim3((kHid / 16) * (kHid / 8), ys), 32, 0, s>>>(d + (size_t)n * kHid, kHid, kHid, h, kHid, kHid, n, slice, grad + oW2,
-                                                                 grad + ob2);
-  k_pred_wgrad<<<dim3((kHid / 16) * (kIn / 8), ys), 32, 0, s>>>(d, kHid, kHid, x, kIn, kIn, n, slice, grad + oW1, grad + ob1);
   return cudaGetLastError();
 }
 cudaError_t rsx_launch_pred_adam(float* w, void* wb, float* m, float* v, const float* grad, float lr, float b1, float b2, float eps, float c1,

@@ -1,6 +1,6 @@
-// The contact predictor's inference on the 5th-generation tensor cores: the 48 -> 128 -> 128 -> 128 -> 6 MLP forward
-// for tiles of 128 arenas with tcgen05.mma (BF16 operands from shared memory, FP32 accumulators in tensor memory),
-// the epilogues (bias, ReLU, BF16) read back with tcgen05.ld.  Same parameters and outputs as k_pred_forward (the
+// The contact predictor on the 5th-generation tensor cores: the 48 -> 128 -> 128 -> 128 -> 6 MLP forward for tiles
+// of 128 arenas with tcgen05.mma (BF16 operands from shared memory, FP32 accumulators in tensor memory), the epilogues
+// (bias, ReLU, BF16) read back with tcgen05.ld; and training's backward through the layers and weight gradients, below.  Same parameters and outputs as k_pred_forward (the
 // mma.sync version), including the saved activations that training's backward pass reads; the logits agree to FP32
 // rounding of the same BF16 products.
 //
@@ -338,6 +338,156 @@ cudaError_t rsx_launch_pred_backward_tc(const void* wb, const float* logits, con
   const uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
   k_pred_backward_tc<<<grid, kRows, kBwdSmemBytes, s>>>((const __nv_bfloat16*)wb, logits, Y, (const __nv_bfloat16*)save, n, inv_scale,
                                                         (__nv_bfloat16*)dz, (__nv_bfloat16*)dsave, loss_sum, err);
+  return cudaGetLastError();
+}
+
+// ---- weight gradients on tcgen05: dW[o][i] += sum_b G[b][o] Act[b][i] and db[o] += sum_b G[b][o] over a slice of
+// the batch, the batch as the MMA's K (64 arenas per staged chunk, both operands transposed into K-major tiles while
+// staging).  The 128-wide side is the MMA's M: o for W3, W2, W1 (G = dH3, dH2, dH1; N = i = 128, 128, 48), i for W4
+// (A = H3, B = dZ with N = 16, so D holds dW4 transposed).  Partial sums of each slice are added with atomics. ----
+namespace {
+constexpr uint32_t kChunk = 64;                      // batch rows per staged chunk (MMA K 64 = 4 instructions)
+constexpr uint32_t gA = 0, gABytes = kRows * kChunk * 2;
+constexpr uint32_t gB = gA + gABytes, gBBytes = kRows * kChunk * 2;
+constexpr uint32_t gMisc = gB + gBBytes;
+constexpr uint32_t kWgradSmemBytes = 56 * 1024;      // at most 4 CTAs per SM: their 128 TMEM columns each always fit
+static_assert(gMisc + 16 + 1024 <= kWgradSmemBytes, "wgrad shared memory");
+}  // namespace
+
+extern "C" __global__ void __launch_bounds__(kRows) k_pred_wgrad_tc(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ dz,
+                                                                    const __nv_bfloat16* __restrict__ save, const __nv_bfloat16* __restrict__ dsave,
+                                                                    uint32_t n, uint32_t slice, float* __restrict__ grad, uint32_t* err) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + gMisc + 8);
+  const uint32_t mbar = sbase + gMisc;
+  const int layer = blockIdx.y;  // 0: W4, 1: W3, 2: W2, 3: W1
+  // A operand (the 128-wide side) and B operand sources: element (row r, batch b) = src[b * stride + r]
+  const __nv_bfloat16* asrc;
+  const __nv_bfloat16* bsrc;
+  uint32_t bstride, N, nb_live;  // B row count in the MMA (N), B rows that exist in the source
+  float* dW;
+  float* db;
+  if (layer == 0) {
+    asrc = save + (size_t)2 * n * kHid;  // H3
+    bsrc = dz;
+    bstride = kOutPad;
+    N = kOutMma;
+    nb_live = kOut;
+    dW = grad + oW4;
+    db = grad + ob4;
+  } else {
+    asrc = dsave + (size_t)(3 - layer) * n * kHid;  // dH3, dH2, dH1
+    bsrc = layer == 3 ? X : save + (size_t)(2 - layer) * n * kHid;  // H2, H1, X
+    bstride = layer == 3 ? kIn : kHid;
+    N = layer == 3 ? kIn : kHid;
+    nb_live = N;
+    dW = grad + (layer == 1 ? oW3 : layer == 2 ? oW2 : oW1);
+    db = grad + (layer == 1 ? ob3 : layer == 2 ? ob2 : ob1);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + gMisc + 8), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t b_lo = blockIdx.x * slice, b_hi = min(n, b_lo + slice);
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  uint32_t phase = 0;
+  bool ok = true, first = true;
+  float bias_acc = 0.0f;  // layers 1..3: db of row o = tid
+  float bias_w4 = 0.0f;   // layer 0: this thread's share of db4[tid % 16]
+#pragma unroll 1
+  for (uint32_t c = b_lo; c < b_hi && ok; c += kChunk) {
+    // stage the chunk, transposing: A element (r, b) for r < 128, B element (r, b) for r < N
+    for (uint32_t idx = tid; idx < (uint32_t)kRows * kChunk; idx += kRows) {
+      const uint32_t b = idx / kRows, r = idx % kRows, gb = c + b;
+      __nv_bfloat16 v = gb < b_hi ? asrc[(size_t)gb * kHid + r] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(sm + gA + canon(r, b, kChunk)) = v;
+      if (layer != 0) bias_acc += __bfloat162float(v);
+    }
+    for (uint32_t idx = tid; idx < N * kChunk; idx += kRows) {
+      const uint32_t b = idx / N, r = idx % N, gb = c + b;
+      __nv_bfloat16 v = (gb < b_hi && r < nb_live) ? bsrc[(size_t)gb * bstride + r] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(sm + gB + canon(r, b, kChunk)) = v;
+      if (layer == 0) bias_w4 += __bfloat162float(v);
+    }
+    fence_smem_to_async();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (tid == 0) {
+      const uint32_t sbo = kChunk / 8 * 128;
+#pragma unroll 1
+      for (uint32_t s = 0; s < kChunk / 16; ++s)
+        mma_bf16(tmem, smem_desc(sbase + gA + s * 256, 128, sbo), smem_desc(sbase + gB + s * 256, 128, sbo), instr_desc(kRows, N),
+                 (first && s == 0) ? 0u : 1u);
+      mma_commit(mbar);
+    }
+    first = false;
+    __syncwarp();
+    if (!__syncthreads_and(mbar_wait(mbar, phase) ? 1 : 0)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    fence_after();
+  }
+  if (ok && !first) {
+    // this thread's accumulator row r = tid: W3 / W2 / W1 row o = r (columns i); W4 column i = r (rows o = columns)
+    const uint32_t lane_base = (warp * 32u) << 16;
+#pragma unroll 1
+    for (uint32_t c0 = 0; c0 < N; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + lane_base + c0, v);
+      for (int j = 0; j < 16; ++j) {
+        const uint32_t col = c0 + j;
+        if (layer == 0) {
+          if (col < (uint32_t)kOut) atomicAdd(&dW[col * kHid + tid], v[j]);
+        } else if (col < N) {
+          atomicAdd(&dW[tid * N + col], v[j]);
+        }
+      }
+    }
+  }
+  if (layer != 0) {
+    atomicAdd(&db[tid], bias_acc);
+  } else {
+    // thread tid staged the dZ column tid % 16 (N = 16 divides 128)
+    if (tid % kOutMma < (uint32_t)kOut) atomicAdd(&db[tid % kOutMma], bias_w4);
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1u);
+    mbar_wait(mbar, phase);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+cudaError_t rsx_launch_pred_wgrads_tc(const void* X, const void* dz, const void* save, const void* dsave, uint32_t n, float* grad, uint32_t* err,
+                                      cudaStream_t s) {
+  static int configured[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !configured[dev]) {
+    e = cudaFuncSetAttribute((const void*)k_pred_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWgradSmemBytes);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) configured[dev] = 1;
+  }
+  const uint32_t slice = 512, slices = (n + slice - 1) / slice;
+  k_pred_wgrad_tc<<<dim3(slices, 4), kRows, kWgradSmemBytes, s>>>((const __nv_bfloat16*)X, (const __nv_bfloat16*)dz, (const __nv_bfloat16*)save,
+                                                                  (const __nv_bfloat16*)dsave, n, slice, grad, err);
   return cudaGetLastError();
 }
 
