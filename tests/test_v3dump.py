@@ -4,6 +4,7 @@ same messages.  Inputs are states of the synthetic world at tick boundaries (sta
 the middle of ticks (after the narrowphase, with contact records, and after the island phase), stepped by the
 library's host build of the simulator."""
 import ctypes
+import json
 import os
 import struct
 import sys
@@ -56,6 +57,44 @@ def cases(rsx):
                 if k >= 4:
                     out.append((s.copy(), sd, f"mid-tick after phase {k} {presets} {a}"))
     return out
+
+
+def golden_states(rsx):
+    """(label, state words, static words) of the pinned dumps: two start states, one after two decisions, one after the
+    narrowphase of the next tick (contact records live), of one car pairing."""
+    L = rsx.lib()
+    sd = rsx.build_static(7, 4, 6)
+    st = rsx.make_states(sd, 6, 11, rsx.MIX_CONTACT_HEAVY)
+    out = [("start 0", st[0].copy(), sd), ("start 1", st[1].copy(), sd)]
+    for d in range(2):
+        ctl = rsx.decision_controls(11, d, 6)
+        for a in range(6):
+            L.rsx_host_decide(_p(st[a]), _p(sd), _p(np.ascontiguousarray(ctl[a])))
+    out.append(("after 2 decisions, arena 2", st[2].copy(), sd))
+    s = st[3].copy()
+    for k in range(5):
+        L.rsx_host_phase(k, _p(s), _p(sd))
+    out.append(("after the narrowphase, arena 3", s, sd))
+    return out
+
+
+def test_dumps_match_the_pinned_hashes(rsx):
+    """The committed sha256 of dumps of fixed states (tests/golden/make_v3_golden.py): both implementations reproduce them."""
+    import hashlib
+
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "v3dump.json")) as f:
+        pinned = json.load(f)
+    for (label, s, sd), want in zip(golden_states(rsx), pinned["arena"]):
+        t = rsx.V3Template()
+        t.config_hash, t.ball_other_set = 0x1234, 1
+        got = rsx.v3_write_arena(s, sd, t)
+        assert want["case"] == label and hashlib.sha256(got).hexdigest() == want["sha256"], label
+        to = O.empty_template()
+        to.update({"config_hash": 0x1234, "ball_other_set": True})
+        assert hashlib.sha256(O.write_arena(s, sd, to)).hexdigest() == want["sha256"], label
+    sb = rsx.v3_write_static(_full_static(rsx))
+    assert hashlib.sha256(sb).hexdigest() == pinned["static"]["sha256"]
+    assert f"{rsx.v3_config_hash(_full_static(rsx)):016x}" == pinned["static"]["config_hash"]
 
 
 def test_fnv1a64_published_vectors(rsx):
