@@ -94,6 +94,8 @@ def lib() -> ctypes.CDLL:
         L.rsx_sim8_multi_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, vp]
         L.rsx_sim8_persistent_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                               ctypes.c_uint32, vp]
+        L.rsx_sim8_persistent_ex.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         L.rsx_sim8_lockstep_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, vp]
         L.rsx_copy_raw.argtypes = [vp, vp, ctypes.c_uint64, vp]

@@ -4,9 +4,11 @@ decisions, and the autotuner that picks the launch configuration.
 A `DecisionRunner` owns the device buffers of one batch of arenas (AoSoA-32 states, per-arena car pairing, results,
 event words, queue counter, arena order, predictor features and logits) and issues one decision with `step()`:
 
-  plain     k_sim8_multi, one thread per arena, one launch per decision (the reference's sim8 shape, block 32)
-  lockstep  the SM-lockstep persistent kernel (rsx_sim8_lockstep_raw) over the identity order
-  binned    the same kernel over the contact predictor's order: features -> MLP -> heavy/quiet bins -> order
+  plain       k_sim8_multi, one thread per arena, one launch per decision (the reference's sim8 shape, block 32)
+  persistent  the persistent kernel without barriers (rsx_sim8_persistent_ex): register budget and queue granularity
+  lockstep    the SM-lockstep persistent kernel (rsx_sim8_lockstep_raw) over the identity order
+  binned      the same kernel over the contact predictor's order: features -> MLP -> heavy/quiet bins -> order
+  levels      the same kernel over the predictor's cost levels: features -> MLP -> 16 expected-contact levels -> order
 
 Every configuration computes the same words (no cross-arena arithmetic), so the autotuner may pick any of them by
 time alone; `tune()` restores the same start states before each candidate so that all candidates step identical work.
@@ -75,6 +77,11 @@ class DecisionRunner:
         if c["mode"] == "plain":
             rsx.check(L.rsx_sim8_multi_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
                                            self.ev.data_ptr(), c.get("block", 32), self.sptr), "rsx_sim8_multi_raw")
+            return
+        if c["mode"] == "persistent":  # the persistent kernel without barriers: register budget, queue granularity
+            rsx.check(L.rsx_sim8_persistent_ex(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
+                                               self.ev.data_ptr(), None, self.counter.data_ptr(), c["grid"], c["block"], c["granularity"],
+                                               c["min_blocks"], None, self.sptr), "rsx_sim8_persistent_ex")
             return
         order = None
         if c["mode"] == "levels":
@@ -154,6 +161,9 @@ class DecisionRunner:
     def candidates(self, binning: bool = True):
         # the plain launch too: with few arenas per SM (a few thousand arenas) the barriers cost more than they save
         out = [{"mode": "plain", "block": 32}, {"mode": "plain", "block": 64}]
+        # the persistent kernel without barriers: register budget (min_blocks of 64 threads per SM) and queue granularity
+        for min_blocks, gran in ((8, 1), (8, 4), (12, 1)):
+            out.append({"mode": "persistent", "block": 64, "grid": self.sms * min_blocks, "granularity": gran, "min_blocks": min_blocks})
         for block, split in itertools.product((448, 512), (6, 7)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
             if binning and self.pred is not None:
