@@ -92,9 +92,11 @@ int rsx_identity(rsx_device* dev, const uint32_t* d_in, uint32_t* d_out, uint32_
  * Per-arena car pairing: d_static points at `count` StaticData, sd_index[a] (u8, device memory) selects arena a's. */
 int rsx_sim8_multi_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                        const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, uint32_t block, void* stream);
-/* The persistent kernel: `grid` resident blocks pull work items (`granularity` arenas) from device queues; with
- * d_bins non-null, arenas are taken bin by bin (bins from rsx_bin_arenas), so warps step arenas of like cost.
- * Results do not depend on grid, block, granularity or binning (no cross-arena arithmetic). */
+/* The persistent kernel: `grid` resident blocks pull work items (32 x `granularity` arenas per warp) from a device
+ * queue: entries of d_order (identity when null; a binned order puts arenas of like predicted cost together) claimed
+ * with atomics on d_queue_counter (cleared by the call).  At most 2^24 arenas, granularity 256 and grid 65,535 per call
+ * (RSX_E_ARG beyond: the 32-bit counter must not wrap).  Results do not depend on grid, block, granularity or order
+ * (no cross-arena arithmetic). */
 int rsx_sim8_persistent_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                             const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or,
                             const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid, uint32_t block,
@@ -113,8 +115,8 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
  * each car's pre-tick inside P1; split 2 splits each car's P1 into pre-tick head, wheel rays and wheel response; split 3 adds a barrier
  * after every step of P3b's pair / leaf loop; split 4 / 5 drop the barriers from P3b / P4 to P8 (slower: kept for
  * measurement); split 6 is split 2 with P5 (rows, iterations, integration) and P8 (cars, the rest) in parts; split 7 is
- * split 6 with P3a one dynamic body at a time.  Register budget by block: up to 448 threads 144 registers, 512 128.  Results
- * equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
+ * split 6 with P3a one dynamic body at a time.  Register budget by block: up to 448 threads 144 registers, 512 128.  At
+ * most 2^24 arenas and grid 65,535 per call.  Results equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
 #define RSX_LOCKSTEP_MAX_BLOCK 512u
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                           const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
@@ -124,8 +126,8 @@ int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics,
  * device memory (their framework owns it, or cudaMalloc / cudaFree would synchronise a real-time loop), the work-queue
  * counter lives in a fixed 256-byte device array of the library instead of d_queue_counter.  At most 2^24 arenas,
  * granularity 256 and grid 65,535 per call (RSX_E_ARG beyond).  The first call on a device looks the array up (make it
- * before any stream capture); calls share the array, so calls whose launches overlap on the GPU race.  Results equal
- * rsx_sim8_persistent_raw's. */
+ * before any stream capture), and so does the first call after a device reset; calls share the array, so calls whose
+ * launches overlap on the GPU race.  Results equal rsx_sim8_persistent_raw's. */
 int rsx_sim8_persistent_noalloc(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                                 const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
                                 uint32_t grid, uint32_t block, uint32_t granularity, void* stream);

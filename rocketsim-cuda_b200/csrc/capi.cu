@@ -248,8 +248,14 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
                            uint32_t block, uint32_t granularity, uint32_t min_blocks, uint32_t* d_cost, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_MAX_BLOCK || (block & 31) ||
       grid == 0 || granularity == 0)
-    return RSX_E_ARG;
-  if (min_blocks != 1 && min_blocks != 8 && min_blocks != 12 && min_blocks != 16) return RSX_E_ARG;
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_persistent_ex: null buffer, or block not 32/64, or grid / granularity 0");
+  if (min_blocks != 1 && min_blocks != 8 && min_blocks != 12 && min_blocks != 16)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_persistent_ex: min_blocks not 1, 8, 12 or 16");
+  // the 32-bit queue counter ends at most grid x block x granularity claims past n: it must not wrap
+  if (n > kQueueMaxArenas || granularity > kQueueMaxGran || grid > kQueueMaxGrid ||
+      (uint64_t)n + (uint64_t)grid * block * granularity >= (1ull << 32))
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_persistent_ex: at most 16,777,216 arenas, granularity 256 and grid 65,535 per call "
+                                         "(the 32-bit queue counter must not wrap)");
   if (n == 0) return RSX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
@@ -274,6 +280,10 @@ int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics,
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
       (block & 31) || grid == 0 || split > 8)
     return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 8");
+  // idle warps claim 32 entries once per tick until their block ends: n plus that overshoot must stay below 2^32
+  if (n > kQueueMaxArenas || grid > kQueueMaxGrid)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: at most 16,777,216 arenas and grid 65,535 per call "
+                                         "(the 32-bit queue counter must not wrap)");
   if (n == 0) return RSX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));

@@ -74,4 +74,25 @@ __device__ __forceinline__ uint32_t decide_arena(uint32_t* states, const StaticD
   return r | (ovf ? kOverflow : 0u);
 }
 
+// The claim loop of the persistent kernels without barriers: each warp takes 32 * gran consecutive entries of `order`
+// (arena indices; identity when null) with one atomicAdd on `counter` (zero at launch) until a claim starts past n, and
+// runs `arena(a)` for each entry below n whose arena index is below n.  The counter overshoots n by at most gridDim.x * blockDim.x * gran, which the
+// launchers keep below 2^32 - n.
+template <class Arena>
+__device__ __forceinline__ void persistent_claims(uint32_t* counter, uint32_t n, uint32_t gran, const uint32_t* order, const Arena& arena) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u * gran);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (base >= n) break;
+    for (uint32_t g = 0; g < gran; ++g) {
+      uint32_t i = base + g * 32u + lane;
+      uint32_t a = i < n ? (order ? order[i] : i) : n;
+      if (a < n) arena(a);  // an order entry past n (not a permutation) is skipped, never dereferenced
+    }
+  }
+}
+
 }  // namespace
+

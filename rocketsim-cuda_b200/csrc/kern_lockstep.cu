@@ -15,7 +15,7 @@
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
 // launch) whenever its previous 32 arenas have finished their 8 ticks, and loads them at the next tick boundary.  The
-// block leaves when no warp holds work.  Lanes past n step a copy of their warp's first arena and store nothing.
+// block leaves when no warp holds work.  Lanes past n (and order entries past n) step a copy of an arena and store nothing.
 //
 // Results: each arena's decision is the decide() sequence of sim/physics.cuh (controls before every tick, all 8 ticks
 // stepped, the state after the first scored tick kept, event OR up to that tick), so states, result words and event
@@ -54,6 +54,10 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         live = i < n;
         uint32_t j = live ? i : base;
         a = order ? order[j] : j;
+        if (a >= n) {  // an order entry past n (not a permutation): step arena 0 as a copy and store nothing
+          a = 0;
+          live = false;
+        }
         D = sds + (sd_index ? sd_index[a] : 0);
         load_tick(&s, states, a);
         c0 = controls[(size_t)a * kCars];

@@ -14,8 +14,10 @@
 // arenas.  Calls on one stream are ordered and safe.
 //
 // Set-up: the first call on a device (the device current at the call) looks up the array's device address with
-// cudaGetSymbolAddress and keeps it; make that first call before any stream capture on the device.  The caller's current
-// device must be the one that holds the buffers and the stream.
+// cudaGetSymbolAddress and keeps it, with the unique ID of the device's CUDA context; make that first call before any
+// stream capture on the device.  A later call whose current context has another ID (the device was reset, which
+// reloads the module, possibly at another address) looks the address up again, so make the first call after a reset
+// before any capture too.  The caller's current device must be the one that holds the buffers and the stream.
 //
 // Limit: at most kNoallocMaxArenas (2^24) arenas per call, granularity at most 256 and grid at most 65,535, so that the
 // 32-bit counter, which overshoots n by up to grid x block x granularity claims, cannot wrap.
@@ -25,9 +27,9 @@
 
 namespace {
 constexpr uint32_t kNoallocScratchWords = 64;
-constexpr uint32_t kNoallocMaxArenas = 1u << 24;
-constexpr uint32_t kNoallocMaxGran = 256;
-constexpr uint32_t kNoallocMaxGrid = 65535;
+constexpr uint32_t kNoallocMaxArenas = kQueueMaxArenas;
+constexpr uint32_t kNoallocMaxGran = kQueueMaxGran;
+constexpr uint32_t kNoallocMaxGrid = kQueueMaxGrid;
 constexpr int kNoallocMaxDevices = 64;
 }  // namespace
 
@@ -39,39 +41,54 @@ extern "C" __global__ void __launch_bounds__(kMaxBlock, 1) k_sim8_persistent_noa
                                                                                      const uint8_t* sd_index, const Controls* controls,
                                                                                      uint32_t* result, uint32_t* ev_or, const uint32_t* order,
                                                                                      uint32_t* counter, uint32_t n, uint32_t gran) {
-  const uint32_t lane = threadIdx.x & 31u;
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(counter, 32u * gran);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    for (uint32_t g = 0; g < gran; ++g) {
-      uint32_t i = base + g * 32u + lane;
-      if (i < n) {
-        uint32_t a = order ? order[i] : i;
-        const StaticData& D = sds[sd_index ? sd_index[a] : 0];
-        result[a] = decide_arena(states, D, controls, a, nullptr, 0, ev_or);
-      }
-    }
-  }
+  persistent_claims(counter, n, gran, order, [&](uint32_t a) {
+    const StaticData& D = sds[sd_index ? sd_index[a] : 0];
+    result[a] = decide_arena(states, D, controls, a, nullptr, 0, ev_or);
+  });
 }
 
 static std::mutex g_noalloc_mu;
 static uint32_t* g_noalloc_ptr[kNoallocMaxDevices];
+static unsigned long long g_noalloc_ctx[kNoallocMaxDevices];
 
-// The scratch array's device address on the current device, looked up once per device (cudaGetSymbolAddress; in host
-// code the array's name is only a host-side stand-in, never a device address).
+// The unique ID of the calling thread's current CUDA context (cuCtxGetCurrent + cuCtxGetId through the runtime's driver
+// entry points, so the library needs no link to the driver library); 0 when there is none or the driver lacks the call.
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+static unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+    (void)cudaGetLastError();
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
+
+// The scratch array's device address on the current device (cudaGetSymbolAddress; in host code the array's name is only
+// a host-side stand-in, never a device address): looked up by the first call on the device, and again when the current
+// context is no longer the one it was looked up in.
 static cudaError_t noalloc_scratch(uint32_t** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev] || current_context_id() != g_noalloc_ctx[dev]) {
     uint32_t* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_noalloc_ptr[dev] = p;
+    g_noalloc_ctx[dev] = current_context_id();  // the lookup made the device's context current
   }
   *out = g_noalloc_ptr[dev];
   return cudaSuccess;

@@ -20,23 +20,12 @@ extern "C" __global__ void __launch_bounds__(kMaxBlock, RSX_MINB) K_NAME(uint32_
                                                                         const Controls* controls, uint32_t* result, uint32_t* ev_or,
                                                                         const uint32_t* order, uint32_t* counter, uint32_t n,
                                                                         uint32_t gran, uint32_t* cost) {
-  const uint32_t lane = threadIdx.x & 31u;
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(counter, 32u * gran);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    for (uint32_t g = 0; g < gran; ++g) {
-      uint32_t i = base + g * 32u + lane;
-      if (i < n) {
-        uint32_t a = order ? order[i] : i;
-        const StaticData& D = sds[sd_index ? sd_index[a] : 0];
-        long long t0 = clock64();
-        result[a] = decide_arena(states, D, controls, a, nullptr, 0, ev_or);
-        if (cost) cost[a] = (uint32_t)((clock64() - t0) >> 8);
-      }
-    }
-  }
+  persistent_claims(counter, n, gran, order, [&](uint32_t a) {
+    const StaticData& D = sds[sd_index ? sd_index[a] : 0];
+    long long t0 = clock64();
+    result[a] = decide_arena(states, D, controls, a, nullptr, 0, ev_or);
+    if (cost) cost[a] = (uint32_t)((clock64() - t0) >> 8);
+  });
 }
 
 cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result, uint32_t* ev_or,

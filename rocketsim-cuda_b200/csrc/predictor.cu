@@ -291,7 +291,8 @@ extern "C" __global__ void __launch_bounds__(1024) k_pred_bin_scatter(const floa
     qb += warp_quiet[w];
   }
   uint32_t below = (1u << lane) - 1u;
-  order[heavy ? hb + __popc(mh & below) : qb + __popc(mq & below)] = a;
+  uint32_t at = heavy ? hb + __popc(mh & below) : qb + __popc(mq & below);
+  if (at < n) order[at] = a;  // always true when both passes read the same logits
 }
 
 // ---- cost levels: an arena's expected contact count e = sum_k w_k * sigmoid(logit_k) over the six outputs, quantised
@@ -365,7 +366,8 @@ extern "C" __global__ void __launch_bounds__(1024) k_pred_level_scatter(const fl
   if (!live) return;
   uint32_t at = base[lv];
   for (uint32_t w = 0; w < warp; ++w) at += warp_cnt[w][lv];
-  order[at + __popc(mine & ((1u << lane) - 1u))] = a;
+  at += __popc(mine & ((1u << lane) - 1u));
+  if (at < n) order[at] = a;  // always true when all three passes read the same logits
 }
 
 // ---- launchers ----

@@ -23,6 +23,15 @@ extern __device__ unsigned long long rsx_zone_acc[148 * 16][64];
       atomicAdd(&rsx_zone_acc[(blockIdx.x * 16u + (threadIdx.x >> 5)) % (148u * 16u)][id],               \
                 (unsigned long long)(clock64() - v));                                                    \
   } while (0)
+#elif defined(RSX_HOST_ZONE_COUNTS) && !defined(__CUDA_ARCH__)
+// Host profiling builds (RSX_HOST_ZONE_COUNTS defined): each marker's end counts one run of its zone in
+// rsx_zone_count[id] of the calling thread, which the including translation unit defines; how often each piece of
+// work runs per arena and tick, for the work-distribution statistics of the decision kernels.
+extern thread_local unsigned long long rsx_zone_count[64];
+#define RSX_ZONE_BEGIN(v) \
+  do {                    \
+  } while (0)
+#define RSX_ZONE_END(v, id) (rsx_zone_count[id] += 1)
 #else
 #define RSX_ZONE_BEGIN(v) \
   do {                    \

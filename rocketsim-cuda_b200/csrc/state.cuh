@@ -241,6 +241,13 @@ constexpr uint32_t kScoredMask = 0xFFu;
 constexpr uint32_t kUnimplemented = 0x80000000u;
 constexpr uint32_t kOverflow = 0x40000000u;
 
+// launch limits of the queue-driven kernels: the 32-bit queue counter must not wrap (n plus the overshoot of the last
+// claims; the lockstep kernel's idle warps claim once per tick); 2^24 arenas are 187 GB of AoSoA state, more than a GPU
+// holds
+constexpr uint32_t kQueueMaxArenas = 1u << 24;
+constexpr uint32_t kQueueMaxGran = 256;
+constexpr uint32_t kQueueMaxGrid = 65535;
+
 // AoSoA-32: word w of arena a at (a / 32) * 32 * kArenaWords + w * 32 + a % 32
 constexpr uint32_t kLanes = 32;
 RSX_F size_t aosoa_block_words() { return (size_t)kArenaWords * kLanes; }

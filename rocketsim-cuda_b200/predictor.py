@@ -112,6 +112,19 @@ class ContactPredictor:
         rsx.check(self.L.rsx_pred_labels_raw(d_event_or, n, Y.data_ptr(), self.stream), "rsx_pred_labels_raw")
         return Y
 
+    def on_stream(self, stream) -> "ContactPredictor":
+        """The same network (weights and optimiser state shared, not copied) issuing its kernels on `stream`.  A caller
+        whose other kernels run on another stream must use such a view: the binning and level orders are counting sorts
+        in two or three passes over the logits, and logits written on one stream while a pass on another reads them can
+        place an arena past the end of the order.  Train through one view only (the Adam step count is the view's)."""
+        import copy
+
+        self.torch.cuda.synchronize(self.device)  # what this view's stream issued so far is done before the other starts
+        v = copy.copy(self)
+        v.stream = stream
+        v._scratch, v._scratch_n = None, 0
+        return v
+
     # ---- network ----
     def logits(self, X, n: int, out=None):
         """Inference on the tensor cores (tcgen05: rsx_pred_forward_tc_raw)."""

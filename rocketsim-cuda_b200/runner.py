@@ -4,6 +4,7 @@ decisions, and the autotuner that picks the launch configuration.
 A `DecisionRunner` owns the device buffers of one batch of arenas (AoSoA-32 states, per-arena car pairing, results,
 event words, queue counter, arena order, predictor features and logits) and issues one decision with `step()`:
 
+  sim8        k_sim8 through rsx_sim8_raw: the reference's sim8 entry (one StaticData for all arenas, block 32)
   plain       k_sim8_multi, one thread per arena, one launch per decision (the reference's sim8 shape, block 32)
   persistent  the persistent kernel without barriers (rsx_sim8_persistent_ex): register budget and queue granularity
   lockstep    the SM-lockstep persistent kernel (rsx_sim8_lockstep_raw) over the identity order
@@ -74,6 +75,10 @@ class DecisionRunner:
         c = config or self.config
         L = rsx.lib()
         n = self.n
+        if c["mode"] == "sim8":  # the reference-shaped entry point: the first StaticData for every arena
+            rsx.check(L.rsx_sim8_raw(self.ds.ptr(), n, self.dsd.ptr(), controls_ptr, self.res.data_ptr(), c.get("block", 32), None,
+                                     self.sptr), "rsx_sim8_raw")
+            return
         if c["mode"] == "plain":
             rsx.check(L.rsx_sim8_multi_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
                                            self.ev.data_ptr(), c.get("block", 32), self.sptr), "rsx_sim8_multi_raw")
@@ -126,6 +131,11 @@ class DecisionRunner:
         rsx.check(rsx.lib().rsx_copy_raw(self.ds.ptr(), buf.data_ptr(), rsx.aosoa_words(self.n) * 4, self.sptr), "rsx_copy_raw")
 
     # ---- the learned part ----
+    def use_predictor(self, pred) -> None:
+        """Takes a predictor trained elsewhere (another runner's, say), bound to this runner's stream so that its
+        kernels stay ordered with this runner's features, binning passes and decisions."""
+        self.pred = None if pred is None else pred.on_stream(self.sptr)
+
     def train_predictor(self, control_seed: int, decisions: int = 32, epochs: int = 6, seed: int = 0, lr: float = 2e-3):
         """Labels from `decisions` exact decisions of these arenas (controls of `control_seed`, run on a snapshot that is
         restored afterwards), then Adam over them; returns (samples, last losses)."""
@@ -174,14 +184,15 @@ class DecisionRunner:
         return out
 
     def tune(self, controls_ptrs, candidates=None, repeats: int = 1):
-        """Times every candidate on the same decisions from the same start states; keeps the fastest as self.config.
-        Returns [(ms, config)] sorted by time."""
+        """Times every candidate on the same decisions from the same start states, `repeats` times each (the candidates
+        interleaved round by round, so that a slow stretch of the machine does not fall on one candidate); keeps the
+        fastest by best time as self.config.  Returns [(best ms, config, [ms of every repeat])] sorted by best time."""
         t = self.torch
         snap = self.snapshot()
-        results = []
-        for c in candidates or self.candidates():
-            best = None
-            for _ in range(repeats):
+        cands = list(candidates or self.candidates())
+        times = [[] for _ in cands]
+        for _ in range(repeats):
+            for i, c in enumerate(cands):
                 self.restore(snap)
                 e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
                 e0.record(self.stream)
@@ -189,12 +200,10 @@ class DecisionRunner:
                     self.step(cp, c)
                 e1.record(self.stream)
                 e1.synchronize()
-                ms = e0.elapsed_time(e1)
-                best = ms if best is None else min(best, ms)
-            results.append((best, c))
+                times[i].append(e0.elapsed_time(e1))
         self.restore(snap)
         self.stream.synchronize()
-        results.sort(key=lambda r: r[0])
+        results = sorted(((min(ts), c, ts) for ts, c in zip(times, cands)), key=lambda r: r[0])
         self.config = dict(results[0][1])
         return results
 

@@ -32,6 +32,23 @@ def test_bad_arguments_are_rejected(rsx):
     assert L.rsx_static_upload(None, None, 1, None) == -1
 
 
+def test_queue_limits_are_refused_before_any_launch(rsx):
+    """The queue-driven entry points refuse sizes whose 32-bit queue counter could wrap (a granularity of 2^27 would
+    make every claim step 32 x granularity wrap to zero, so the warps would never leave), with a message and before any
+    CUDA call: dummy non-null pointers are never touched."""
+    L = rsx.lib()
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    L.rsx_sim8_persistent_ex.argtypes = [vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, u32, u32, vp, vp]
+    L.rsx_sim8_lockstep_raw.argtypes = [vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, u32, vp]
+    p = vp(256)
+    for n, grid, block, gran in ((1000, 148, 32, 1 << 27), (1000, 148, 32, 257), (1000, 65536, 32, 1), ((1 << 24) + 1, 148, 32, 1)):
+        assert L.rsx_sim8_persistent_ex(p, n, p, None, p, p, None, None, p, grid, block, gran, 1, None, None) == -1, (n, grid, gran)
+        assert b"wrap" in L.rsx_last_error() or b"granularity" in L.rsx_last_error()
+    for n, grid in (((1 << 24) + 1, 148), (1000, 65536)):
+        assert L.rsx_sim8_lockstep_raw(p, n, p, None, p, p, None, None, p, grid, 448, 7, None) == -1
+        assert b"wrap" in L.rsx_last_error()
+
+
 @pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
 def test_no_device_is_reported(rsx):
     L = rsx.lib()

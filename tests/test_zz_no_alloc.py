@@ -62,9 +62,11 @@ def test_noalloc_matches_persistent_on_two_calls(rsx):
                      dev.stream_ptr())
         assert rc == -1
         assert b"16,777,216" in L.rsx_last_error()
-        rc = noalloc(new_states.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), new_res.data_ptr(), None, None, 148, 32, 257,
-                     dev.stream_ptr())
-        assert rc == -1
+        # granularity past 256, grid past 65,535, a block that is not 32 or 64: refused the same way
+        for grid, block, gran in ((148, 32, 257), (65536, 32, 1), (148, 96, 1)):
+            rc = noalloc(new_states.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), new_res.data_ptr(), None, None, grid, block, gran,
+                         dev.stream_ptr())
+            assert rc == -1, (grid, block, gran)
         dev.sync()
         assert np.array_equal(dev.download_words(new_states), got)
         for h in (ref_states, new_states, dsd):
