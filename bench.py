@@ -79,7 +79,8 @@ def kernel_name(config):
     if m == "persistent":
         return f"k_sim8_persistent_b{config['min_blocks']}"
     t = 448 if config["block"] <= 448 else 512
-    return f"k_sim8_lockstep_t{t}<{config['split']}>"
+    name = f"k_sim8_lockstep_t{t}<{config['split']}>"
+    return name if config.get("ticks", 8) == 8 else f"{name} x{8 // config['ticks']} launches"
 
 
 def parse():
@@ -585,7 +586,9 @@ def run_ours(args):
 
     # ---- roofline of the decision kernel (HBM: algorithmic bytes per launch / launch time) ----
     mean_ms = t_ms / args.steps
-    alg_bytes = n * 8 * ALG_BYTES_PER_ARENA_TICK
+    launches = 8 // config.get("ticks", 8) if config["mode"] in ("lockstep", "binned", "levels") else 1
+    # state in and out, controls and result words once per launch of the decision
+    alg_bytes = n * launches * (2 * TICK_BYTES + 64 + 4)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -601,7 +604,7 @@ def run_ours(args):
                 "traffic_unit": f"bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of {kname}, {kc['capture']})" if kc else
                 f"no ncu capture of {kname} in profiles/",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "kernel": kname,
-                "algorithmic_bytes_per_launch": alg_bytes, "kernel_ms_per_launch": mean_ms}
+                "algorithmic_bytes_per_decision": alg_bytes, "launches_per_decision": launches, "kernel_ms_per_decision": mean_ms}
     sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
     clk_hz = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
     warp_issue_peak = sms * 4 * clk_hz  # 4 schedulers per SM issue one warp instruction per cycle each

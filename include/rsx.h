@@ -121,6 +121,16 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
                           const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
                           uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t split, void* stream);
+/* The same decision in 8 / ticks_per_launch launches of ticks_per_launch ticks each (1, 2, 4 or 8; no counterpart in
+ * the reference, whose step_ticks takes the tick count, arena_step.cuh:83-105): every launch re-claims the arenas from
+ * the queue, and each arena's progress between launches rides in d_result (scored tick, RSX_UNIMPLEMENTED) and
+ * d_event_or (the event OR so far); an arena scored in an earlier launch is not stepped again and keeps its goal state.
+ * The words after the last launch equal rsx_sim8_lockstep_raw's.  A tuning knob: with several claim rounds, shorter
+ * launches re-balance the arenas across SMs more often. */
+int rsx_sim8_lockstep_ex(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,
+                         const rsx_controls* d_controls, uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order,
+                         uint32_t* d_queue_counter, uint32_t grid, uint32_t block, uint32_t split, uint32_t ticks_per_launch,
+                         void* stream);
 
 /* The persistent decision without caller scratch (no counterpart in the reference): for callers that cannot allocate
  * device memory (their framework owns it, or cudaMalloc / cudaFree would synchronise a real-time loop), the work-queue

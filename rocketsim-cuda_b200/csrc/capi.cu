@@ -24,7 +24,8 @@ RSX_DECL_PERSIST(16)
 #define RSX_DECL_LOCKSTEP(T)                                                                                                \
   cudaError_t rsx_launch_sim8_lockstep_t##T(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls,         \
                                             uint32_t* result, uint32_t* ev_or, const uint32_t* order, uint32_t* counter, uint32_t n,  \
-                                            uint32_t grid, uint32_t block, int split, cudaStream_t s);
+                                            uint32_t grid, uint32_t block, int split, uint32_t t_first, uint32_t t_last,                \
+                                            cudaStream_t s);
 RSX_DECL_LOCKSTEP(448)
 RSX_DECL_LOCKSTEP(512)
 cudaError_t rsx_launch_pred_features(const uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t n,
@@ -277,24 +278,36 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
                           uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
                           uint32_t block, uint32_t split, void* stream) {
+  return rsx_sim8_lockstep_ex(d_states, n, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, grid, block,
+                              split, RSX_TICKS_PER_DECISION, stream);
+}
+
+int rsx_sim8_lockstep_ex(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const rsx_controls* d_controls,
+                         uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
+                         uint32_t block, uint32_t split, uint32_t ticks_per_launch, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
       (block & 31) || grid == 0 || split > 8)
-    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 8");
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep: null buffer, block not a multiple of 32 in 32..512, grid 0 or split > 8");
+  if (ticks_per_launch == 0 || RSX_TICKS_PER_DECISION % ticks_per_launch != 0)
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_ex: ticks_per_launch must divide 8 (1, 2, 4 or 8)");
   // idle warps claim 32 entries once per tick until their block ends: n plus that overshoot must stay below 2^32
   if (n > kQueueMaxArenas || grid > kQueueMaxGrid)
-    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_raw: at most 16,777,216 arenas and grid 65,535 per call "
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep: at most 16,777,216 arenas and grid 65,535 per call "
                                          "(the 32-bit queue counter must not wrap)");
   if (n == 0) return RSX_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
-  cudaError_t e;
-  if (block <= 448)
-    e = rsx_launch_sim8_lockstep_t448(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
-                                      block, (int)split, s);
-  else
-    e = rsx_launch_sim8_lockstep_t512(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
-                                      block, (int)split, s);
-  RSX_CK(e);
+  for (uint32_t t0 = 1; t0 <= RSX_TICKS_PER_DECISION; t0 += ticks_per_launch) {
+    const uint32_t t1 = t0 + ticks_per_launch - 1;
+    RSX_CK(cudaMemsetAsync(d_queue_counter, 0, 4, s));
+    cudaError_t e;
+    if (block <= 448)
+      e = rsx_launch_sim8_lockstep_t448(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
+                                        block, (int)split, t0, t1, s);
+    else
+      e = rsx_launch_sim8_lockstep_t512(d_states, d_statics, d_sd_index, d_controls, d_result, d_event_or, d_order, d_queue_counter, n, grid,
+                                        block, (int)split, t0, t1, s);
+    RSX_CK(e);
+  }
   return RSX_OK;
 }
 

@@ -14,7 +14,10 @@
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
-// launch) whenever its previous 32 arenas have finished their 8 ticks, and loads them at the next tick boundary.  The
+// launch) whenever its previous 32 arenas have finished this launch's ticks (t_first..t_last of the decision's 8), and
+// loads them at the next tick boundary.  A decision split over several launches carries each arena's progress in its
+// result word (scored tick, unimplemented bit) and event word; an arena scored in an earlier launch is not stepped
+// again.  The
 // block leaves when no warp holds work.  Lanes past n (and order entries past n) step a copy of an arena and store nothing.
 //
 // Results: each arena's decision is the decide() sequence of sim/physics.cuh (controls before every tick, all 8 ticks
@@ -36,7 +39,8 @@
 template <int SPLIT>
 __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const StaticData* sds, const uint8_t* sd_index,
                                                         const Controls* controls, uint32_t* result, uint32_t* ev_or,
-                                                        const uint32_t* order, uint32_t* counter, uint32_t n) {
+                                                        const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t t_first,
+                                                        uint32_t t_last) {
   const uint32_t lane = threadIdx.x & 31u;
   ArenaState s;
   Controls c0, c1;
@@ -62,8 +66,15 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         load_tick(&s, states, a);
         c0 = controls[(size_t)a * kCars];
         c1 = controls[(size_t)a * kCars + 1];
-        t = 1;
+        t = t_first;
         scored = unimpl = ev = 0;
+        if (t_first > 1) {  // a later launch of a split decision: the progress so far rides in the result / event words
+          uint32_t r0 = result[a];
+          scored = r0 & kScoredMask;
+          unimpl = r0 & kUnimplemented;
+          ev = ev_or ? ev_or[a] : 0u;
+          if (scored) live = false;  // decided in an earlier launch (the buffer holds its goal state): store nothing
+        }
         ovf = false;
         have = true;
       }
@@ -202,7 +213,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           ovf = sim::any_overflow(s);
         }
       }
-      if (t == kTicksPerDecision) {
+      if (t == t_last) {  // the end of this launch's ticks (tick 8: of the decision)
         if (scored == 0) {
           if (live) store_tick(states, a, &s);
           ovf = sim::any_overflow(s);
@@ -219,26 +230,22 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
 }
 
 cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, const void* controls, uint32_t* result, uint32_t* ev_or,
-                   const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, cudaStream_t s) {
+                   const uint32_t* order, uint32_t* counter, uint32_t n, uint32_t grid, uint32_t block, int split, uint32_t t_first,
+                   uint32_t t_last, cudaStream_t s) {
   const StaticData* D = (const StaticData*)sds;
   const Controls* C = (const Controls*)controls;
-  if (split == 8)
-    K_NAME<8><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 7)
-    K_NAME<7><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 6)
-    K_NAME<6><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 5)
-    K_NAME<5><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 4)
-    K_NAME<4><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 3)
-    K_NAME<3><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split == 2)
-    K_NAME<2><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else if (split)
-    K_NAME<1><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
-  else
-    K_NAME<0><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n);
+#define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
+  switch (split) {
+    case 8: RSX_LS_LAUNCH(8); break;
+    case 7: RSX_LS_LAUNCH(7); break;
+    case 6: RSX_LS_LAUNCH(6); break;
+    case 5: RSX_LS_LAUNCH(5); break;
+    case 4: RSX_LS_LAUNCH(4); break;
+    case 3: RSX_LS_LAUNCH(3); break;
+    case 2: RSX_LS_LAUNCH(2); break;
+    case 1: RSX_LS_LAUNCH(1); break;
+    default: RSX_LS_LAUNCH(0); break;
+  }
+#undef RSX_LS_LAUNCH
   return cudaGetLastError();
 }

@@ -981,12 +981,20 @@ RSX_F int near_head(Ctx& c, uint32_t rb0, uint32_t rb1, NearPair& np, BoxJob& bj
   return NEAR_DONE;
 }
 
-// P3b driver: pairs in order; a mesh pair's leaves one by one, each leaf's contact added in order.  The loop is kept
-// as a state (P3bLoop) and a step (one leaf of the current mesh job, or the next pairs up to one that opens a job), so
-// that a kernel can step the loops of many arenas in lockstep; phase3b runs the steps to the end.
+// P3b driver: pairs in order; a mesh pair's leaves in BVH walk order, each leaf's contact added in that order.  The loop
+// is kept as a state (P3bLoop) and a step, so that a kernel can step the loops of many arenas in lockstep; phase3b runs
+// the steps to the end.  A step runs the pair heads up to the next mesh job (or the end of the pairs), then one chunk of
+// the open job: up to kLeafChunk leaves taken from the walk, tested, and their hits added in walk order; the job's tail
+// follows the chunk that exhausts the walk.  Taking the leaves of a chunk before testing them, and testing them before
+// adding any, computes what the reference's leaf-by-leaf loop computes (collision_dispatcher.cuh:240-280): the walk
+// reads only the job's fixed query box and the static BVH, and a leaf's test reads only the job's fixed transforms and
+// the static triangle, so neither depends on the contacts added before it; only the additions are ordered.  Kernels can
+// therefore run the tests of a chunk on any lanes (p3b_collect, leaf_test, p3b_add_hit, p3b_close below).
+constexpr int kLeafChunk = 32;
 struct P3bLoop {
   uint32_t n, i, unimplemented;
   int kind;
+  bool walk_done;  // the open job's walk has no leaf left
   NearPair np;
   BoxJob bj;
   SphereJob sj;
@@ -996,82 +1004,172 @@ RSX_F void p3b_begin(const ArenaState& S, P3bLoop& L) {
   L.i = 0;
   L.unimplemented = 0;
   L.kind = NEAR_DONE;
+  L.walk_done = false;
   L.np = NearPair{};
 }
-// one step; false when the phase has no work left
-RSX_F bool p3b_step(ArenaState& S, const StaticData& D, P3bLoop& L) {
-  if (!(L.kind != NEAR_DONE || L.i < L.n)) return false;
+RSX_F bool p3b_more(const P3bLoop& L) { return L.kind != NEAR_DONE || L.i < L.n; }
+
+// The pair heads up to the next mesh job: returns its kind (NEAR_BOX_JOB / NEAR_SPHERE_JOB), or NEAR_DONE when the pairs
+// ran out.  A job already open is returned as it is.
+RSX_F int p3b_open(ArenaState& S, const StaticData& D, P3bLoop& L) {
+  if (L.kind != NEAR_DONE) return L.kind;
   Ctx c = {S, D, L.unimplemented};
-  NearPair& np = L.np;
-  BoxJob& bj = L.bj;
-  SphereJob& sj = L.sj;
-  if (L.kind == NEAR_DONE) {
-    RSX_ZONE_BEGIN(z_head);
-    while (L.i < L.n) {
-      Pair p = S.pairs[L.i++];
-      L.kind = near_head(c, D.proxies[p.h0].body, D.proxies[p.h1].body, np, bj, sj);
-      if (L.kind != NEAR_DONE) break;
-    }
-    RSX_ZONE_END(z_head, 10);
-    if (L.kind == NEAR_DONE) {
-      L.unimplemented = c.unimplemented;
-      return false;
-    }
+  RSX_ZONE_BEGIN(z_head);
+  while (L.i < L.n) {
+    Pair p = S.pairs[L.i++];
+    L.kind = near_head(c, D.proxies[p.h0].body, D.proxies[p.h1].body, L.np, L.bj, L.sj);
+    if (L.kind != NEAR_DONE) break;
   }
-  uint32_t tri;
+  RSX_ZONE_END(z_head, 10);
+  L.unimplemented = c.unimplemented;
+  L.walk_done = false;
+  return L.kind;
+}
+
+// The next leaves of the open job's walk (at most cap) into tris[], in walk order; sets L.walk_done when the walk ends.
+RSX_F int p3b_collect(const StaticData& D, P3bLoop& L, uint32_t* tris, int cap) {
+  int k = 0;
+  while (k < cap) {
+    uint32_t tri;
+    bool more;
+    if (L.kind == NEAR_BOX_JOB) {
+      RSX_ZONE_BEGIN(z_bnext);
+      more = box_job_next(D, L.bj, &tri);
+      RSX_ZONE_END(z_bnext, 12);
+    } else {
+      RSX_ZONE_BEGIN(z_snext);
+      more = cursor_next(L.sj.cu, D, *L.sj.mesh, L.sj.box, &tri);
+      RSX_ZONE_END(z_snext, 14);
+    }
+    if (!more) {
+      L.walk_done = true;
+      break;
+    }
+    tris[k++] = tri;
+  }
+  return k;
+}
+
+// What one leaf's test needs, fixed for the whole job: the box job's car box and the mesh-to-box transform, or the
+// sphere job's centre (in the mesh's frame) and radii; and where the mesh's triangles start.
+struct LeafJob {
+  int kind;
+  uint32_t tri_first;
+  Aff box_xf, mesh_to_box;
+  V3 half;
+  float margin, maxd;
+  V3 center;
+  float radius, rt, rt2;
+};
+// One leaf's result: box jobs use point (the contact in world) and depth (the distance); sphere jobs normal, point
+// (in the mesh's frame) and depth.
+struct LeafHit {
+  uint32_t found;
+  V3 normal, point;
+  float depth;
+};
+RSX_F void leaf_job_of(const P3bLoop& L, LeafJob& j) {
+  j.kind = L.kind;
   if (L.kind == NEAR_BOX_JOB) {
-    RSX_ZONE_BEGIN(z_bnext);
-    bool more = box_job_next(D, bj, &tri);
-    RSX_ZONE_END(z_bnext, 12);
-    if (more) {
-      RSX_ZONE_BEGIN(z_sat);
-      const Tri& t = D.tris[bj.mesh->tri_first + tri];
-      V3 q[3] = {xform_point(bj.mesh_to_box, t.p0), xform_point(bj.mesh_to_box, t.p1), xform_point(bj.mesh_to_box, t.p2)};
-      SatHit h;
-      if (box_triangle_sat(bj.box_xf, bj.half, bj.margin, q, bj.maxd, &h)) {
-        if (!bj.has_m) {
-          bj.m = manifold_new(bj.car, bj.mesh_body);
-          bj.has_m = true;
-        }
-        add_contact(c, bj.m, bj.car, bj.mesh_body, bj.tri_rot * t.n, h.point_world, h.distance, (int32_t)tri);
-      }
-      RSX_ZONE_END(z_sat, 11);
-    } else {
-      RSX_ZONE_BEGIN(z_btail);
-      Manifold fresh = {};
-      bool has = false;
-      if (bj.has_m) {
-        refresh_points(S, D, bj.m, bj.car, bj.mesh_body);
-        if (bj.m.n != 0) {
-          fresh = bj.m;
-          has = true;
-        }
-      }
-      near_tail(c, np.rb0, np.rb1, np.cached, has, fresh);
-      L.kind = NEAR_DONE;
-      RSX_ZONE_END(z_btail, 13);
-    }
+    j.tri_first = L.bj.mesh->tri_first;
+    j.box_xf = L.bj.box_xf;
+    j.mesh_to_box = L.bj.mesh_to_box;
+    j.half = L.bj.half;
+    j.margin = L.bj.margin;
+    j.maxd = L.bj.maxd;
   } else {
-    RSX_ZONE_BEGIN(z_snext);
-    bool more = cursor_next(sj.cu, D, *sj.mesh, sj.box, &tri);
-    RSX_ZONE_END(z_snext, 14);
-    if (more) {
-      RSX_ZONE_BEGIN(z_stri);
-      SphereTriHit h;
-      if (sphere_triangle(D.tris[sj.mesh->tri_first + tri], sj.center, sj.radius, sj.rt, sj.rt2, &h))
-        add_contact(c, S.manifolds[sj.manifold], sj.sph, sj.mesh_body, h.normal, h.point + sj.mesh_t, h.depth, (int32_t)tri);
-      RSX_ZONE_END(z_stri, 15);
-    } else {
-      RSX_ZONE_BEGIN(z_stail);
-      Manifold& m = S.manifolds[sj.manifold];
-      if (m.n != 0) refresh_points(S, D, m, sj.sph, sj.mesh_body);
-      push_active(S, (uint32_t)sj.manifold);
-      L.kind = NEAR_DONE;
-      RSX_ZONE_END(z_stail, 16);
+    j.tri_first = L.sj.mesh->tri_first;
+    j.center = L.sj.center;
+    j.radius = L.sj.radius;
+    j.rt = L.sj.rt;
+    j.rt2 = L.sj.rt2;
+  }
+}
+// The test of one leaf (a pure function of the job and the static triangle).
+RSX_F bool leaf_test(const LeafJob& j, const StaticData& D, uint32_t tri, LeafHit* h) {
+  const Tri& t = D.tris[j.tri_first + tri];
+  if (j.kind == NEAR_BOX_JOB) {
+    RSX_ZONE_BEGIN(z_sat);
+    V3 q[3] = {xform_point(j.mesh_to_box, t.p0), xform_point(j.mesh_to_box, t.p1), xform_point(j.mesh_to_box, t.p2)};
+    SatHit sh;
+    bool f = box_triangle_sat(j.box_xf, j.half, j.margin, q, j.maxd, &sh);
+    h->found = f;
+    h->point = sh.point_world;
+    h->depth = sh.distance;
+    RSX_ZONE_END(z_sat, 11);
+    return f;
+  }
+  RSX_ZONE_BEGIN(z_stri);
+  SphereTriHit sh;
+  bool f = sphere_triangle(t, j.center, j.radius, j.rt, j.rt2, &sh);
+  h->found = f;
+  h->normal = sh.normal;
+  h->point = sh.point;
+  h->depth = sh.depth;
+  RSX_ZONE_END(z_stri, 15);
+  return f;
+}
+// The contact of a leaf whose test found one, into the job's manifold (in walk order).
+RSX_F void p3b_add_hit(ArenaState& S, const StaticData& D, P3bLoop& L, uint32_t tri, const LeafHit& h) {
+  Ctx c = {S, D, L.unimplemented};
+  if (L.kind == NEAR_BOX_JOB) {
+    BoxJob& bj = L.bj;
+    const Tri& t = D.tris[bj.mesh->tri_first + tri];
+    if (!bj.has_m) {
+      bj.m = manifold_new(bj.car, bj.mesh_body);
+      bj.has_m = true;
     }
+    add_contact(c, bj.m, bj.car, bj.mesh_body, bj.tri_rot * t.n, h.point, h.depth, (int32_t)tri);
+  } else {
+    SphereJob& sj = L.sj;
+    add_contact(c, S.manifolds[sj.manifold], sj.sph, sj.mesh_body, h.normal, h.point + sj.mesh_t, h.depth, (int32_t)tri);
   }
   L.unimplemented = c.unimplemented;
-  return L.kind != NEAR_DONE || L.i < L.n;
+}
+// The job's tail once its walk is done: the box job's fresh manifold merged into the pair's (or inserted), the sphere
+// job's manifold refreshed and marked active.
+RSX_F void p3b_close(ArenaState& S, const StaticData& D, P3bLoop& L) {
+  Ctx c = {S, D, L.unimplemented};
+  if (L.kind == NEAR_BOX_JOB) {
+    RSX_ZONE_BEGIN(z_btail);
+    BoxJob& bj = L.bj;
+    Manifold fresh = {};
+    bool has = false;
+    if (bj.has_m) {
+      refresh_points(S, D, bj.m, bj.car, bj.mesh_body);
+      if (bj.m.n != 0) {
+        fresh = bj.m;
+        has = true;
+      }
+    }
+    near_tail(c, L.np.rb0, L.np.rb1, L.np.cached, has, fresh);
+    RSX_ZONE_END(z_btail, 13);
+  } else {
+    RSX_ZONE_BEGIN(z_stail);
+    SphereJob& sj = L.sj;
+    Manifold& m = S.manifolds[sj.manifold];
+    if (m.n != 0) refresh_points(S, D, m, sj.sph, sj.mesh_body);
+    push_active(S, (uint32_t)sj.manifold);
+    RSX_ZONE_END(z_stail, 16);
+  }
+  L.kind = NEAR_DONE;
+  L.unimplemented = c.unimplemented;
+}
+
+// one step; false when the phase has no work left
+RSX_F bool p3b_step(ArenaState& S, const StaticData& D, P3bLoop& L) {
+  if (!p3b_more(L)) return false;
+  if (p3b_open(S, D, L) == NEAR_DONE) return false;
+  uint32_t tris[kLeafChunk];
+  int k = p3b_collect(D, L, tris, kLeafChunk);
+  LeafJob j;
+  leaf_job_of(L, j);
+  for (int i = 0; i < k; ++i) {
+    LeafHit h;
+    if (leaf_test(j, D, tris[i], &h)) p3b_add_hit(S, D, L, tris[i], h);
+  }
+  if (L.walk_done) p3b_close(S, D, L);
+  return p3b_more(L);
 }
 
 RSX_F uint32_t phase3b(ArenaState& S, const StaticData& D) {

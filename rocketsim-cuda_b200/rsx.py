@@ -98,6 +98,8 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         L.rsx_sim8_lockstep_raw.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                             ctypes.c_uint32, vp]
+        L.rsx_sim8_lockstep_ex.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.c_uint32, ctypes.c_uint32, vp]
         L.rsx_copy_raw.argtypes = [vp, vp, ctypes.c_uint64, vp]
         L.rsx_make_states_at.argtypes = [u32p, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float), u32p]
         L.rsx_l2_persist_raw.argtypes = [vp, ctypes.c_uint64, ctypes.c_float, vp]

@@ -7,7 +7,8 @@ event words, queue counter, arena order, predictor features and logits) and issu
   sim8        k_sim8 through rsx_sim8_raw: the reference's sim8 entry (one StaticData for all arenas, block 32)
   plain       k_sim8_multi, one thread per arena, one launch per decision (the reference's sim8 shape, block 32)
   persistent  the persistent kernel without barriers (rsx_sim8_persistent_ex): register budget and queue granularity
-  lockstep    the SM-lockstep persistent kernel (rsx_sim8_lockstep_raw) over the identity order
+  lockstep    the SM-lockstep persistent kernel (rsx_sim8_lockstep_ex) over the identity order, 8 / `ticks` launches
+              of `ticks` ticks per decision (default 8: one launch)
   binned      the same kernel over the contact predictor's order: features -> MLP -> heavy/quiet bins -> order
   levels      the same kernel over the predictor's cost levels: features -> MLP -> 16 expected-contact levels -> order
 
@@ -107,15 +108,16 @@ class DecisionRunner:
             rsx.check(p.L.rsx_pred_bin_raw(self.Z.data_ptr(), n, thr, c.get("labels", P.ALL_LABELS), self.bin_scratch.data_ptr(),
                                            self.order.data_ptr(), self.heavy.data_ptr(), self.sptr), "bin")
             order = self.order.data_ptr()
-        rsx.check(L.rsx_sim8_lockstep_raw(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
-                                          self.ev.data_ptr(), order, self.counter.data_ptr(), c.get("grid", self.sms), c["block"],
-                                          c["split"], self.sptr), "rsx_sim8_lockstep_raw")
+        rsx.check(L.rsx_sim8_lockstep_ex(self.ds.ptr(), n, self.dsd.ptr(), self.didx.data_ptr(), controls_ptr, self.res.data_ptr(),
+                                         self.ev.data_ptr(), order, self.counter.data_ptr(), c.get("grid", self.sms), c["block"],
+                                         c["split"], c.get("ticks", 8), self.sptr), "rsx_sim8_lockstep_ex")
 
     def kernels_per_step(self, config: dict | None = None) -> int:
         """This library's kernel launches per decision (features, forward, two binning passes or three level passes,
-        the decision)."""
+        and the decision's launches: 8 / ticks per launch for the lockstep kernel)."""
         c = config or self.config
-        return {"binned": 5, "levels": 6}.get(c["mode"], 1)
+        launches = 8 // c.get("ticks", 8) if c["mode"] in ("lockstep", "binned", "levels") else 1
+        return {"binned": 4, "levels": 5}.get(c["mode"], 0) + launches
 
     # ---- states ----
     def snapshot(self):
@@ -176,6 +178,9 @@ class DecisionRunner:
             out.append({"mode": "persistent", "block": 64, "grid": self.sms * min_blocks, "granularity": gran, "min_blocks": min_blocks})
         for block, split in itertools.product((448, 512), (6, 7)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
+            if split == 7:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
+                for ticks in (4, 2):
+                    out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None, "ticks": ticks})
             if binning and self.pred is not None:
                 for thr, labels in ((0.3, P.ALL_LABELS), (0.5, P.ALL_LABELS)):
                     out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr, "labels": labels})

@@ -150,6 +150,46 @@ def test_result_independent_of_block_order_and_queue(rsx, dev):
         assert np.array_equal(ref[:, :rsx.TICK_WORDS], outs[0][0][:, :rsx.TICK_WORDS])
 
 
+def test_ticks_per_launch_same_words(rsx, dev):
+    """A decision split over 2, 4 or 8 launches of the lockstep kernel (rsx_sim8_lockstep_ex; progress carried in the
+    result and event words, arenas re-claimed between launches) gives the words of the one-launch decision: states,
+    result words (goals included: a scored arena keeps its goal state through the later launches) and event words, over
+    several claim rounds (grid 2) and one (grid 148), identity and permuted orders."""
+    import torch
+
+    sds = np.stack([rsx.build_static(7, p, q) for p, q in [(0, 0), (2, 6)]])
+    n = 1000
+    idx = (np.arange(n) % 2).astype(np.uint8)
+    st = rsx.make_states_multi(sds, idx, 17, rsx.MIX_CONTACT_HEAVY)
+    dsd = dev.upload_static(sds)
+    didx = torch.from_numpy(idx).to(dev.device)
+    perm = torch.from_numpy(np.random.default_rng(4).permutation(n).astype(np.int32)).to(dev.device)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
+    L = rsx.lib()
+    outs = []
+    for ticks, grid, order, block in ((8, 148, None, 448), (4, 148, None, 448), (2, 2, perm, 448), (1, 148, perm, 512), (4, 3, None, 64)):
+        ds = dev.upload_states(st)
+        res = dev.alloc_result(n)
+        ev = torch.zeros(n, dtype=torch.int32, device=dev.device)
+        scored = 0
+        for d in range(6):
+            ctl = dev.upload_controls(rsx.decision_controls(13, d, n))
+            rsx.check(L.rsx_sim8_lockstep_ex(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), ev.data_ptr(),
+                                             order.data_ptr() if order is not None else None, counter.data_ptr(), grid, block, 7, ticks,
+                                             dev.stream_ptr()), f"lockstep ticks {ticks}")
+            dev.sync()
+            scored += int(((res.cpu().numpy().view(np.uint32) & 0xFF) != 0).sum())
+        outs.append((dev.download_states(ds)[:, :rsx.TICK_WORDS], res.cpu().numpy(), ev.cpu().numpy(), scored))
+        ds.free()
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+        assert np.array_equal(o[1], outs[0][1])
+        assert np.array_equal(o[2], outs[0][2])
+    assert outs[0][3] > 0, "the case should hold goals (a scored arena must keep its goal state across launches)"
+    assert L.rsx_sim8_lockstep_ex(None, n, dsd.ptr(), None, None, None, None, None, None, 148, 448, 7, 3, None) == -1
+    dsd.free()
+
+
 def test_trace_and_tick_kernels_match_oracle(rsx, dev, world):
     import torch
 
