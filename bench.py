@@ -103,9 +103,9 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=7,
+    ap.add_argument("--split", type=int, default=9,
                     help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts, "
-                         "7 = 6 + P3a per body")
+                         "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain launch's comparison timing")
     ap.add_argument("--no-oracle", action="store_true", help="skip the word-for-word replay through the oracle")
@@ -535,7 +535,7 @@ def run_ours(args):
         Zs, Ys = [], []
         with torch.cuda.stream(run.stream):  # the copies on the stream the kernels wrote on
             for s in range(leg.steps):
-                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 7, "threshold": 0.5})
+                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 9, "threshold": 0.5})
                 Zs.append(run.Z.clone())
                 Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         run.stream.synchronize()
@@ -748,9 +748,9 @@ def large_leg(args, dev, pred, L):
 
 def profile_variants(args, leg):
     """For an ncu capture at the headline size: for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 6 / 7), two decisions and then the captured one, each from the same start states."""
+    (blocks 448 / 512, splits 7 / 9), two decisions and then the captured one, each from the same start states."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (6, 7)]
+                                                   for b in (448, 512) for s in (7, 9)]
     out = []
     for cfg in variants:
         leg.run.restore(leg.start)
@@ -788,7 +788,7 @@ def sweep(args, dev):
         t0 = time.perf_counter()
         run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
         train_s = time.perf_counter() - t0
-        base = {"block": 448, "grid": run.sms, "split": 7}
+        base = {"block": 448, "grid": run.sms, "split": 9}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
                           ("binned", {"mode": "binned", "threshold": 0.5, **base}),

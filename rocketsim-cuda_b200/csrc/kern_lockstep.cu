@@ -36,6 +36,115 @@
 #define K_NAME RSX_CAT(k_sim8_lockstep_t, RSX_LS_MAXT)
 #define L_NAME RSX_CAT(rsx_launch_sim8_lockstep_t, RSX_LS_MAXT)
 
+namespace {
+// ---- split 9: P3b with the leaf tests of every arena of the block pooled ----
+// Each round, every lane whose arena has P3b work runs its pair heads up to its next mesh job and takes up to
+// sim::kLeafChunk leaves of the job's BVH walk; the jobs and their (job, leaf) tests are published in shared memory
+// (slots from a block-wide prefix sum); all threads of the block then run the tests, kPoolPairs at most, one test per
+// thread at a time; each owner adds its hits in walk order and closes the job when its walk is done.  A heavy arena's
+// leaves (a ball against a wall: up to ~30 triangles in one tick) are thus tested side by side instead of one after
+// another on one lane, while the order-dependent part (the manifold updates) stays on the owner.  Jobs past the pool's
+// capacity test their own leaves, as in the other splits.  Words equal every other split's: the walk / test / add
+// separation is exact (sim/narrow.cuh, P3b driver).
+constexpr int kPoolJobs = 128;
+constexpr int kPoolPairs = 512;
+struct PoolSmem {
+  sim::LeafJob job[kPoolJobs];
+  const StaticData* jd[kPoolJobs];
+  uint32_t pair_job[kPoolPairs];
+  uint32_t pair_tri[kPoolPairs];
+  sim::LeafHit hit[kPoolPairs];
+  uint32_t warp_sum[32];
+  uint32_t limit;
+};
+
+// block-wide exclusive prefix sum of v (every thread calls it); returns the exclusive sum, *total the block's sum
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, PoolSmem& sm) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+    if (lane >= (uint32_t)d) x += y;
+  }
+  if (lane == 31) sm.warp_sum[warp] = x;
+  if (threadIdx.x == 0) sm.limit = 0;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < nw ? sm.warp_sum[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, d);
+      if (lane >= (uint32_t)d) w += y;
+    }
+    sm.warp_sum[lane] = w;
+  }
+  __syncthreads();
+  *total = sm.warp_sum[nw - 1];
+  return (warp ? sm.warp_sum[warp - 1] : 0u) + x - v;
+}
+
+// P3b of the thread's arena (have) with pooled leaf tests; every thread of the block calls it
+__device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool have, int* un) {
+  __shared__ PoolSmem sm;
+  sim::P3bLoop L;
+  bool more = have;
+  if (have) sim::p3b_begin(s, L);
+  uint32_t tris[sim::kLeafChunk];
+  for (;;) {
+    int k = 0;
+    bool job = false;
+    if (more) {
+      if (sim::p3b_open(s, *D, L) == sim::NEAR_DONE) {
+        more = false;
+      } else {
+        job = true;
+        k = sim::p3b_collect(*D, L, tris, sim::kLeafChunk);
+      }
+    }
+    // (the barrier also orders the last round's reads of the pool before this round's writes)
+    if (!__syncthreads_or(job)) break;
+    uint32_t total;
+    const uint32_t v = k > 0 ? ((1u << 16) | (uint32_t)k) : 0u;
+    const uint32_t ex = block_scan(v, &total, sm);
+    const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
+    // pooled jobs are a prefix in scan order (slot and off only grow), so the pool's pairs are [0, limit)
+    const bool pooled = k > 0 && slot < (uint32_t)kPoolJobs && off + (uint32_t)k <= (uint32_t)kPoolPairs;
+    if (pooled) {
+      sim::leaf_job_of(L, sm.job[slot]);
+      sm.jd[slot] = D;
+      for (int i = 0; i < k; ++i) {
+        sm.pair_job[off + i] = slot;
+        sm.pair_tri[off + i] = tris[i];
+      }
+      atomicMax(&sm.limit, off + (uint32_t)k);
+    }
+    __syncthreads();
+    const uint32_t npairs = sm.limit;
+    for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
+      const uint32_t j = sm.pair_job[p];
+      sim::LeafHit h;
+      sim::leaf_test(sm.job[j], *sm.jd[j], sm.pair_tri[p], &h);
+      sm.hit[p] = h;
+    }
+    __syncthreads();
+    if (pooled) {
+      for (int i = 0; i < k; ++i)
+        if (sm.hit[off + i].found) sim::p3b_add_hit(s, *D, L, tris[i], sm.hit[off + i]);
+    } else if (k > 0) {  // past the pool's capacity: this lane tests its own leaves
+      sim::LeafJob jb;
+      sim::leaf_job_of(L, jb);
+      for (int i = 0; i < k; ++i) {
+        sim::LeafHit h;
+        if (sim::leaf_test(jb, *D, tris[i], &h)) sim::p3b_add_hit(s, *D, L, tris[i], h);
+      }
+    }
+    if (job && L.walk_done) sim::p3b_close(s, *D, L);
+  }
+  if (have && L.unimplemented != 0) *un = 1;
+}
+}  // namespace
+
 template <int SPLIT>
 __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const StaticData* sds, const uint8_t* sd_index,
                                                         const Controls* controls, uint32_t* result, uint32_t* ev_or,
@@ -161,6 +270,10 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           if (bar) __syncthreads();
           continue;
         }
+        if (SPLIT == 9 && k == 4) {  // P3b with the block's leaf tests pooled
+          p3b_pooled(s, D, have, &un);
+          continue;
+        }
         if (SPLIT == 3 && k == 4) {
           // P3b with a barrier after every step of the pair / leaf loop
           sim::P3bLoop L;
@@ -236,6 +349,7 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
   const Controls* C = (const Controls*)controls;
 #define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
   switch (split) {
+    case 9: RSX_LS_LAUNCH(9); break;
     case 8: RSX_LS_LAUNCH(8); break;
     case 7: RSX_LS_LAUNCH(7); break;
     case 6: RSX_LS_LAUNCH(6); break;

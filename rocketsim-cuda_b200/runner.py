@@ -52,7 +52,7 @@ class DecisionRunner:
         self.Z = t.zeros((n, 8), dtype=t.float32, device=dev.device)
         self.sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
         self.pred = None
-        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 6, "threshold": None}
+        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 9, "threshold": None}
         torch.cuda.synchronize(dev.device)
 
     # ---- observations and rewards of the last decision ----
@@ -146,7 +146,7 @@ class DecisionRunner:
             self.pred = P.ContactPredictor(self.dev.device, seed=seed, stream=self.sptr)
         snap = self.snapshot()
         Xs, Ys = [], []
-        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 7}
+        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 9}
         for d in range(decisions):
             ctl = t.from_numpy(rsx.decision_controls(control_seed, d, self.n).view(np.int32)).to(self.dev.device, non_blocking=False)
             self.stream.wait_stream(t.cuda.current_stream(self.dev.device))
@@ -176,9 +176,9 @@ class DecisionRunner:
         # the persistent kernel without barriers: register budget (min_blocks of 64 threads per SM) and queue granularity
         for min_blocks, gran in ((8, 1), (8, 4), (12, 1)):
             out.append({"mode": "persistent", "block": 64, "grid": self.sms * min_blocks, "granularity": gran, "min_blocks": min_blocks})
-        for block, split in itertools.product((448, 512), (6, 7)):
+        for block, split in itertools.product((448, 512), (7, 9)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
-            if split == 7:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
+            if split == 9:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
                 for ticks in (4, 2):
                     out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None, "ticks": ticks})
             if binning and self.pred is not None:

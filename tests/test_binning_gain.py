@@ -44,7 +44,7 @@ def test_trained_order_gain_is_measured_and_exact(rsx):
             e1.synchronize()
             return e0.elapsed_time(e1), run.snapshot().cpu().numpy(), run.res.cpu().numpy().copy()
 
-        base = {"block": 448, "grid": run.sms, "split": 7}
+        base = {"block": 448, "grid": run.sms, "split": 9}
         for_warm = timed({"mode": "lockstep", **base})  # first launches load the kernels
         t_id, w_id, r_id = timed({"mode": "lockstep", **base})
         t_un, w_un, r_un = timed({"mode": "binned", "threshold": 0.5, **base})
