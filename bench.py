@@ -65,6 +65,10 @@ KERNEL_COUNTERS = {
                                 "lanes_active": 11667652598 / 1370835710},
     "k_sim8_lockstep_t512<7>": {"dram_bytes_per_arena": (5456979712 + 5481598208) / _N, "warp_inst_per_arena_tick": 1371659501 / _T,
                                 "lanes_active": 11688968835 / 1371659501},
+    "k_sim8_lockstep_t448<9>": {"dram_bytes_per_arena": 11290000640 / _N, "warp_inst_per_arena_tick": 1345642323 / _T,
+                                "lanes_active": 12233723383 / 1345642323},
+    "k_sim8_lockstep_t512<9>": {"dram_bytes_per_arena": 11303093248 / _N, "warp_inst_per_arena_tick": 1347599346 / _T,
+                                "lanes_active": 12307438977 / 1347599346},
 }
 for _k in KERNEL_COUNTERS.values():
     _k["capture"] = "65,536 arenas, the headline decision 3 (same size as the timed run)"
@@ -120,6 +124,8 @@ def parse():
     ap.add_argument("--sweep-decisions", type=int, default=4)
     ap.add_argument("--zones", action="store_true", help="zone-timer profile instead of the bench line")
     ap.add_argument("--zones-all", action="store_true", help="with --zones: every marker of the simulator")
+    ap.add_argument("--zones-lockstep", action="store_true", help="with --zones: the pieces of the lockstep kernel at --split (block 448)")
+    ap.add_argument("--zones-skip", type=int, default=0, help="with --zones: plain decisions run first (untimed)")
     ap.add_argument("--mix", default="headline", choices=["headline", "contact"])
     ap.add_argument("--profile-variants", action="store_true",
                     help="one decision of the plain launch and of each lockstep variant after two of its own, for an ncu capture")
@@ -848,6 +854,15 @@ for _k, _nm in enumerate(["P0", "P1", "P2", "P3a", "P3b", "P4", "P5", "P6", "P7"
     ZONE_NAMES[50 + _k] = "barrier after " + _nm
 
 
+LOCKSTEP_ZONE_NAMES = {40: "P0", 41: "P1 pre-tick head (per car)", 42: "P1 wheel rays (per car)", 43: "P1 wheel response (per car)",
+                       44: "P2", 45: "P3a (per body)", 46: "P3b", 47: "P4", 48: "P5 (3 pieces)", 49: "P6", 29: "P7", 30: "P8 (2 pieces)",
+                       33: "  P3b heads and walks", 34: "  P3b pooled leaf tests", 35: "  P3b additions and tails",
+                       60: "copy-in (load_tick)", 61: "copy-out (store_tick)"}
+for _i, _nm in zip([50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 31, 32],
+                   ["P0", "P1 head", "P1 rays", "P1 response", "P2", "P3a", "P3b (pool rounds)", "P4", "P5", "P6", "P7", "P8"]):
+    LOCKSTEP_ZONE_NAMES[_i] = "barrier after " + _nm
+
+
 def zones(args, dev):
     """Zone-timer profile of `sweep_decisions` decisions of the workload: warp cycles per phase and per barrier (and with
     --zones-all the simulator's inner markers), from the profiling builds librsx_zones.so / librsx_zones_all.so
@@ -855,9 +870,14 @@ def zones(args, dev):
     import torch
     import rsx
 
-    Z = ctypes.CDLL(os.path.join(ROOT, "rocketsim-cuda_b200", "librsx_zones_all.so" if args.zones_all else "librsx_zones.so"))
+    lib = "librsx_zones_ls.so" if args.zones_lockstep else ("librsx_zones_all.so" if args.zones_all else "librsx_zones.so")
+    Z = ctypes.CDLL(os.path.join(ROOT, "rocketsim-cuda_b200", lib))
     vp = ctypes.c_void_p
-    Z.rsx_zones_decision.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp]
+    if args.zones_lockstep:
+        Z.rsx_zones_lockstep.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_int, vp]
+    else:
+        Z.rsx_zones_decision.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp]
+    names = LOCKSTEP_ZONE_NAMES if args.zones_lockstep else ZONE_NAMES
     n = args.arenas
     sds, idx, st = world(rsx, n, 0, args.seed, rsx.MIX_HEADLINE if args.mix == "headline" else rsx.MIX_CONTACT_HEAVY)
     dsd = dev.upload_static(sds)
@@ -866,19 +886,35 @@ def zones(args, dev):
     res = torch.zeros(n, dtype=torch.int32, device=dev.device)
     counter = torch.zeros(1, dtype=torch.int32, device=dev.device)
     tot = np.zeros(64, np.float64)
-    for d in range(args.sweep_decisions):
+    for d in range(args.zones_skip):  # to the states of later decisions (the bench times decisions after its warm-up)
+        ctl = dev.upload_controls(rsx.decision_controls(1000, d, n))
+        rsx.check(rsx.lib().rsx_sim8_multi_raw(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), None, 32,
+                                               dev.stream_ptr()), "rsx_sim8_multi_raw")
+    dev.sync()
+    for d in range(args.zones_skip, args.zones_skip + args.sweep_decisions):
         ctl = dev.upload_controls(rsx.decision_controls(1000, d, n))
         out = np.zeros(64, np.uint64)
-        rc = Z.rsx_zones_decision(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), counter.data_ptr(), out.ctypes.data)
+        if args.zones_lockstep:
+            rc = Z.rsx_zones_lockstep(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), counter.data_ptr(), 448, args.split,
+                                      out.ctypes.data)
+        else:
+            rc = Z.rsx_zones_decision(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), counter.data_ptr(), out.ctypes.data)
         if rc != 0:
             raise RuntimeError(f"zone run failed ({rc})")
         tot += out.astype(np.float64)
-    phases = sum(tot[40 + k] for k in range(10))
-    barriers = sum(tot[50 + k] for k in range(10))
-    print(f"{args.mix}, {n} arenas, {args.sweep_decisions} decisions: warp Gcycles in phases {phases / 1e9:.2f}, at barriers {barriers / 1e9:.2f}")
-    for i in sorted(ZONE_NAMES):
+    if args.zones_lockstep:
+        pieces = [40, 41, 42, 43, 44, 45, 46, 47, 48, 49, 29, 30]
+        bars = [50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 31, 32]
+    else:
+        pieces, bars = [40 + k for k in range(10)], [50 + k for k in range(10)]
+    phases = sum(tot[i] for i in pieces)
+    barriers = sum(tot[i] for i in bars)
+    allc = phases + barriers
+    print(f"{args.mix}, {n} arenas, {args.sweep_decisions} decisions{', lockstep split %d' % args.split if args.zones_lockstep else ''}: "
+          f"warp Gcycles in phases {phases / 1e9:.2f}, at barriers {barriers / 1e9:.2f}")
+    for i in sorted(names):
         if tot[i] > 0:
-            print(f"  {ZONE_NAMES[i]:28s} {tot[i] / 1e9:9.3f} G  {100 * tot[i] / phases:6.2f}% of phase cycles")
+            print(f"  {names[i]:34s} {tot[i] / 1e9:9.3f} G  {100 * tot[i] / allc:6.2f}% of all warp cycles")
     ds.free()
     dsd.free()
 

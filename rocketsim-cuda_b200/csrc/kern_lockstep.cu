@@ -34,6 +34,15 @@
 #define RSX_CAT2(a, b) a##b
 #define RSX_CAT(a, b) RSX_CAT2(a, b)
 #define K_NAME RSX_CAT(k_sim8_lockstep_t, RSX_LS_MAXT)
+// Zone timers of the profiling build (RSX_ZONES; empty markers otherwise): warp cycles in each piece of the tick
+// (ids 40-49 and 29-30: P0, P1 head, P1 rays, P1 response, P2, P3a, P3b, P4, P5, P6, P7, P8), at the barrier after it
+// (ids 50-59 and 31-32 likewise), and inside the pooled P3b (33 heads and walks, 34 pooled tests, 35 additions).
+#define LS_SYNC(id)          \
+  do {                       \
+    RSX_ZONE_BEGIN(zb_);     \
+    __syncthreads();         \
+    RSX_ZONE_END(zb_, id);   \
+  } while (0)
 #define L_NAME RSX_CAT(rsx_launch_sim8_lockstep_t, RSX_LS_MAXT)
 
 namespace {
@@ -94,6 +103,7 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
   for (;;) {
     int k = 0;
     bool job = false;
+    RSX_ZONE_BEGIN(zo);
     if (more) {
       if (sim::p3b_open(s, *D, L) == sim::NEAR_DONE) {
         more = false;
@@ -102,8 +112,12 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
         k = sim::p3b_collect(*D, L, tris, sim::kLeafChunk);
       }
     }
+    RSX_ZONE_END(zo, 33);
     // (the barrier also orders the last round's reads of the pool before this round's writes)
-    if (!__syncthreads_or(job)) break;
+    RSX_ZONE_BEGIN(zb0);
+    const bool any = __syncthreads_or(job);
+    RSX_ZONE_END(zb0, 56);
+    if (!any) break;
     uint32_t total;
     const uint32_t v = k > 0 ? ((1u << 16) | (uint32_t)k) : 0u;
     const uint32_t ex = block_scan(v, &total, sm);
@@ -119,15 +133,18 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
       }
       atomicMax(&sm.limit, off + (uint32_t)k);
     }
-    __syncthreads();
+    LS_SYNC(56);
     const uint32_t npairs = sm.limit;
+    RSX_ZONE_BEGIN(zt);
     for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
       const uint32_t j = sm.pair_job[p];
       sim::LeafHit h;
       sim::leaf_test(sm.job[j], *sm.jd[j], sm.pair_tri[p], &h);
       sm.hit[p] = h;
     }
-    __syncthreads();
+    RSX_ZONE_END(zt, 34);
+    LS_SYNC(56);
+    RSX_ZONE_BEGIN(zc);
     if (pooled) {
       for (int i = 0; i < k; ++i)
         if (sm.hit[off + i].found) sim::p3b_add_hit(s, *D, L, tris[i], sm.hit[off + i]);
@@ -140,6 +157,7 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
       }
     }
     if (job && L.walk_done) sim::p3b_close(s, *D, L);
+    RSX_ZONE_END(zc, 35);
   }
   if (have && L.unimplemented != 0) *un = 1;
 }
@@ -172,7 +190,9 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           live = false;
         }
         D = sds + (sd_index ? sd_index[a] : 0);
+        RSX_ZONE_BEGIN(zl);
         load_tick(&s, states, a);
+        RSX_ZONE_END(zl, 60);
         c0 = controls[(size_t)a * kCars];
         c1 = controls[(size_t)a * kCars + 1];
         t = t_first;
@@ -196,8 +216,12 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
       s.cars[1].controls = c1;
     }
     if (SPLIT >= 2) {
-      if (have) sim::t_p0(s, *D);
-      __syncthreads();
+      {
+        RSX_ZONE_BEGIN(z0);
+        if (have) sim::t_p0(s, *D);
+        RSX_ZONE_END(z0, 40);
+      }
+      LS_SYNC(50);
       if (have) {
         sim::flip_zdamp(s, *D, 0);
         sim::flip_zdamp(s, *D, 1);
@@ -208,6 +232,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         bool act = false;
         float rthr = 0.0f;
         uint32_t was = 0;
+        RSX_ZONE_BEGIN(z1);
         if (SPLIT == 8) {  // the pre-tick head in three parts
           sim::PreTick pt;
           if (have) {
@@ -222,47 +247,74 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           was = s.cars[ci].on_ground;
           act = sim::car_pre_tick_head(s, *D, ci, &rthr);
         }
-        __syncthreads();
+        RSX_ZONE_END(z1, 41);
+        LS_SYNC(51);
         sim::WheelHit hits[kWheels];
-        if (have && act) sim::vehicle_rays(s, *D, ci, hits);
-        __syncthreads();
-        if (have) {
-          if (act) {
-            sim::vehicle_response(s, *D, ci, sim::kTickTime, s.cars[ci].handbrake_val, rthr, D->cars[ci].three_wheels != 0, hits);
-            sim::car_pre_tick_tail(s, *D, ci);
-          }
-          if (!was && s.cars[ci].on_ground) s.events |= 1u << (EV_LANDED + ci);
+        {
+          RSX_ZONE_BEGIN(z2);
+          if (have && act) sim::vehicle_rays(s, *D, ci, hits);
+          RSX_ZONE_END(z2, 42);
         }
-        __syncthreads();
+        LS_SYNC(52);
+        {
+          RSX_ZONE_BEGIN(z3);
+          if (have) {
+            if (act) {
+              sim::vehicle_response(s, *D, ci, sim::kTickTime, s.cars[ci].handbrake_val, rthr, D->cars[ci].three_wheels != 0, hits);
+              sim::car_pre_tick_tail(s, *D, ci);
+            }
+            if (!was && s.cars[ci].on_ground) s.events |= 1u << (EV_LANDED + ci);
+          }
+          RSX_ZONE_END(z3, 43);
+        }
+        LS_SYNC(53);
       }
 #pragma unroll 1
       for (int k = 2; k < sim::kPhases; ++k) {
         // split 4: no barrier between P3b and P8 (warps without contact work run ahead to the tick's end);
         // split 5: none between P4 and P8
         const bool bar = !((SPLIT == 4 && k >= 4 && k < sim::kPhases - 1) || (SPLIT == 5 && k >= 5 && k < sim::kPhases - 1));
+        // zone ids of phase k's pieces and of the barriers after them
+        const int zp = k <= 7 ? 42 + k : 21 + k, zb = zp + (k <= 7 ? 10 : 2);
+        (void)zp;
+        (void)zb;
         if (SPLIT >= 7 && k == 3) {  // P3a: one dynamic body at a time
 #pragma unroll 1
           for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
-            if (have) sim::t_p3a_body(s, *D, d);
-            __syncthreads();
+            {
+              RSX_ZONE_BEGIN(za);
+              if (have) sim::t_p3a_body(s, *D, d);
+              RSX_ZONE_END(za, zp);
+            }
+            LS_SYNC(zb);
           }
           continue;
         }
         if (SPLIT >= 6 && k == 6) {  // P5: rows, iterations, integration
           sim::Solver sv;
+          RSX_ZONE_BEGIN(z5a);
           if (have) sim::t_p5_setup(s, *D, sv);
-          __syncthreads();
+          RSX_ZONE_END(z5a, zp);
+          LS_SYNC(zb);
+          RSX_ZONE_BEGIN(z5b);
           if (have) sim::t_p5_iterate(sv);
-          __syncthreads();
+          RSX_ZONE_END(z5b, zp);
+          LS_SYNC(zb);
+          RSX_ZONE_BEGIN(z5c);
           if (have) sim::t_p5_finish(s, *D, sv);
-          __syncthreads();
+          RSX_ZONE_END(z5c, zp);
+          LS_SYNC(zb);
           continue;
         }
         if (SPLIT >= 6 && k == 9) {  // P8: cars, then pads / ball / tick count
+          RSX_ZONE_BEGIN(z8a);
           if (have) sim::t_p8_cars(s);
-          __syncthreads();
+          RSX_ZONE_END(z8a, zp);
+          LS_SYNC(zb);
+          RSX_ZONE_BEGIN(z8b);
           if (have) sim::t_p8_rest(s, *D);
-          __syncthreads();
+          RSX_ZONE_END(z8b, zp);
+          LS_SYNC(zb);
           continue;
         }
         if (SPLIT == 4 || SPLIT == 5) {
@@ -284,8 +336,12 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           if (have && L.unimplemented != 0) un = 1;
           continue;
         }
-        if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
-        __syncthreads();
+        {
+          RSX_ZONE_BEGIN(zk);
+          if (have && sim::run_phase(k, s, *D) != sim::PHASE_OK) un = 1;
+          RSX_ZONE_END(zk, zp);
+        }
+        LS_SYNC(zb);
       }
     } else if (SPLIT) {
       if (have) sim::t_p0(s, *D);
@@ -327,10 +383,12 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         }
       }
       if (t == t_last) {  // the end of this launch's ticks (tick 8: of the decision)
+        RSX_ZONE_BEGIN(zs);
         if (scored == 0) {
           if (live) store_tick(states, a, &s);
           ovf = sim::any_overflow(s);
         }
+        RSX_ZONE_END(zs, 61);
         if (live) {
           if (ev_or) ev_or[a] = ev;
           result[a] = scored | unimpl | (ovf ? kOverflow : 0u);
@@ -363,3 +421,27 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
 #undef RSX_LS_LAUNCH
   return cudaGetLastError();
 }
+
+#ifdef RSX_ZONES
+// Zone-timer profiling build (not part of librsx.so): one decision of this kernel with zone sums over all warps.
+__device__ unsigned long long rsx_zone_acc[148 * 16][64];
+extern "C" int rsx_zones_lockstep(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index, const void* d_controls,
+                                  uint32_t* d_result, uint32_t* d_counter, uint32_t block, int split, unsigned long long* zone_cycles) {
+  static unsigned long long acc[148 * 16][64];
+  memset(acc, 0, sizeof(acc));
+  if (cudaMemcpyToSymbol(rsx_zone_acc, acc, sizeof(acc)) != cudaSuccess) return -2;
+  if (cudaMemset(d_counter, 0, 4) != cudaSuccess) return -2;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  if (L_NAME(d_states, d_statics, d_sd_index, d_controls, d_result, nullptr, nullptr, d_counter, n, sms < 148 ? sms : 148, block, split, 1,
+             kTicksPerDecision, 0) != cudaSuccess)
+    return -2;
+  if (cudaDeviceSynchronize() != cudaSuccess) return -2;
+  if (cudaMemcpyFromSymbol(acc, rsx_zone_acc, sizeof(acc)) != cudaSuccess) return -2;
+  for (int z = 0; z < 64; ++z) {
+    zone_cycles[z] = 0;
+    for (int w = 0; w < 148 * 16; ++w) zone_cycles[z] += acc[w][z];
+  }
+  return 0;
+}
+#endif
