@@ -63,12 +63,34 @@ struct PoolSmem {
   uint32_t pair_job[kPoolPairs];
   uint32_t pair_tri[kPoolPairs];
   sim::LeafHit hit[kPoolPairs];
+};
+// split 10: the wheel rays' mesh leaves pooled the same way (sim/ray.cuh: evaluated anywhere, replayed on the owner)
+constexpr int kRayJobs = 64;
+constexpr int kRayPairs = 512;
+constexpr int kRayChunk = 16;
+struct RayPoolSmem {
+  sim::RayMeshJob job[kRayJobs];
+  const StaticData* jd[kRayJobs];
+  uint32_t pair_job[kRayPairs];  // job slot | mesh index << 16
+  uint32_t pair_leaf[kRayPairs];
+  sim::RayLeaf out[kRayPairs];
+};
+// one shared buffer for both pools (they serve different pieces of the tick) and the prefix sums
+struct Pools {
+  union {
+    PoolSmem p3b;
+    RayPoolSmem rays;
+  };
   uint32_t warp_sum[32];
   uint32_t limit;
 };
+__device__ __forceinline__ Pools& pools() {
+  __shared__ Pools u;
+  return u;
+}
 
 // block-wide exclusive prefix sum of v (every thread calls it); returns the exclusive sum, *total the block's sum
-__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, PoolSmem& sm) {
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, Pools& sm) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   uint32_t x = v;
 #pragma unroll
@@ -95,7 +117,8 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, Pool
 
 // P3b of the thread's arena (have) with pooled leaf tests; every thread of the block calls it
 __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool have, int* un) {
-  __shared__ PoolSmem sm;
+  Pools& u = pools();
+  PoolSmem& sm = u.p3b;
   sim::P3bLoop L;
   bool more = have;
   if (have) sim::p3b_begin(s, L);
@@ -120,7 +143,7 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
     if (!any) break;
     uint32_t total;
     const uint32_t v = k > 0 ? ((1u << 16) | (uint32_t)k) : 0u;
-    const uint32_t ex = block_scan(v, &total, sm);
+    const uint32_t ex = block_scan(v, &total, u);
     const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
     // pooled jobs are a prefix in scan order (slot and off only grow), so the pool's pairs are [0, limit)
     const bool pooled = k > 0 && slot < (uint32_t)kPoolJobs && off + (uint32_t)k <= (uint32_t)kPoolPairs;
@@ -131,10 +154,10 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
         sm.pair_job[off + i] = slot;
         sm.pair_tri[off + i] = tris[i];
       }
-      atomicMax(&sm.limit, off + (uint32_t)k);
+      atomicMax(&u.limit, off + (uint32_t)k);
     }
     LS_SYNC(56);
-    const uint32_t npairs = sm.limit;
+    const uint32_t npairs = u.limit;
     RSX_ZONE_BEGIN(zt);
     for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
       const uint32_t j = sm.pair_job[p];
@@ -160,6 +183,99 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
     RSX_ZONE_END(zc, 35);
   }
   if (have && L.unimplemented != 0) *un = 1;
+}
+
+// The wheel rays of car ci of the thread's arena (act) with the mesh leaves of the whole block pooled; every thread of
+// the block calls it.  Each round, every lane runs its candidate bodies in order up to its next mesh body (planes, the
+// ball and the other car are tested in place), sets that body's test up and takes up to kRayChunk leaves of its walk;
+// all threads evaluate the published leaves; each owner replays its leaves in walk order (slab limits, hits) and moves
+// to the next candidate when the walk is done.  Results equal vehicle_rays'.
+__device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, bool act, int ci, sim::WheelHit hits[kWheels]) {
+  Pools& u = pools();
+  RayPoolSmem& sm = u.rays;
+  sim::RayPacket pk;
+  uint32_t cand[kHandles];
+  int nk = 0, kc = 0;
+  if (act) {
+    sim::vehicle_rays_begin(s, *D, ci, pk);
+    nk = sim::grid_candidates(s, *D, &pk, cand);
+  }
+  bool open = false, wdone = false;
+  sim::LocalRays lr;
+  sim::RayBox rb;
+  sim::RayWalk wk;
+  sim::RayMeshJob mj;
+  uint32_t leaves[kRayChunk];
+  int meshes[kRayChunk];
+  for (;;) {
+    int k = 0;
+    if (act) {
+      while (!open && kc < nk) {
+        const uint32_t w = cand[kc];
+        if (D->bodies[w].shape == sim::SHAPE_MESH) {
+          sim::ray_body_setup(s, *D, w, &pk, lr, rb);
+          sim::ray_mesh_job(lr, rb, mj);
+          sim::ray_walk_seek(wk, *D, w, rb.box, 0);
+          open = true;
+          wdone = false;
+        } else {
+          sim::ray_body(s, *D, w, &pk);
+          ++kc;
+        }
+      }
+      if (open) {
+        int mesh;
+        uint32_t leaf;
+        while (k < kRayChunk) {
+          if (!sim::ray_walk_next(wk, *D, cand[kc], rb.box, &mesh, &leaf)) {
+            wdone = true;
+            break;
+          }
+          leaves[k] = leaf;
+          meshes[k] = mesh;
+          ++k;
+        }
+      }
+    }
+    if (!__syncthreads_or(open)) break;
+    uint32_t total;
+    const uint32_t ex = block_scan(k > 0 ? ((1u << 16) | (uint32_t)k) : 0u, &total, u);
+    const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
+    const bool pooled = k > 0 && slot < (uint32_t)kRayJobs && off + (uint32_t)k <= (uint32_t)kRayPairs;
+    if (pooled) {
+      sm.job[slot] = mj;
+      sm.jd[slot] = D;
+      for (int i = 0; i < k; ++i) {
+        sm.pair_job[off + i] = slot | ((uint32_t)meshes[i] << 16);
+        sm.pair_leaf[off + i] = leaves[i];
+      }
+      atomicMax(&u.limit, off + (uint32_t)k);
+    }
+    __syncthreads();
+    const uint32_t npairs = u.limit;
+    for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
+      const uint32_t j = sm.pair_job[p] & 0xFFFFu;
+      const StaticData& Dj = *sm.jd[j];
+      sim::ray_leaf_eval(sm.job[j], Dj, Dj.meshes[sm.pair_job[p] >> 16], sm.pair_leaf[p], nullptr, &sm.out[p]);
+    }
+    __syncthreads();
+    if (open) {
+      for (int i = 0; i < k; ++i) {
+        const MeshInfo& m = D->meshes[meshes[i]];
+        sim::RayLeaf e;
+        if (pooled)
+          e = sm.out[off + i];
+        else  // past the pool's capacity: this lane evaluates its own leaves
+          sim::ray_leaf_eval(mj, *D, m, leaves[i], rb.lmax, &e);
+        sim::ray_leaf_replay(&lr, rb.lmax, *D, m, leaves[i], e);
+      }
+      if (wdone) {
+        open = false;
+        ++kc;
+      }
+    }
+  }
+  if (act) sim::wheel_packet_hits(s, *D, pk, hits);
 }
 }  // namespace
 
@@ -252,7 +368,10 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         sim::WheelHit hits[kWheels];
         {
           RSX_ZONE_BEGIN(z2);
-          if (have && act) sim::vehicle_rays(s, *D, ci, hits);
+          if (SPLIT >= 10)
+            rays_pooled(s, D, have && act, ci, hits);
+          else if (have && act)
+            sim::vehicle_rays(s, *D, ci, hits);
           RSX_ZONE_END(z2, 42);
         }
         LS_SYNC(52);
@@ -322,7 +441,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           if (bar) __syncthreads();
           continue;
         }
-        if (SPLIT == 9 && k == 4) {  // P3b with the block's leaf tests pooled
+        if (SPLIT >= 9 && k == 4) {  // P3b with the block's leaf tests pooled
           p3b_pooled(s, D, have, &un);
           continue;
         }
@@ -407,6 +526,7 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
   const Controls* C = (const Controls*)controls;
 #define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
   switch (split) {
+    case 10: RSX_LS_LAUNCH(10); break;
     case 9: RSX_LS_LAUNCH(9); break;
     case 8: RSX_LS_LAUNCH(8); break;
     case 7: RSX_LS_LAUNCH(7); break;

@@ -220,8 +220,8 @@ RSX_F V3 steered_axle(const Aff& cxf, float angle) {
   return qrotate(quat_axis_sc(cxf.m.c2, s, c), cxf.m.c1);
 }
 
-// the wheels' hard points and the four wheel rays against the world (the first half of vehicle_update)
-RSX_HD RSX_NOINL inline void vehicle_rays(ArenaState& S, const StaticData& D, int ci, WheelHit hits[kWheels]) {
+// the wheels' hard points and the packet of the four wheel rays (the start of vehicle_update's ray query)
+RSX_F void vehicle_rays_begin(ArenaState& S, const StaticData& D, int ci, RayPacket& pk) {
   Car& car = S.cars[ci];
   const CarConst& cc = D.cars[ci];
   const uint32_t cidx = cc.body;
@@ -234,9 +234,16 @@ RSX_HD RSX_NOINL inline void vehicle_rays(ArenaState& S, const StaticData& D, in
     tgt[i] = w.hard_point - (cxf.m.c2 * wc.ray_length);
     src[i] = w.hard_point;
   }
+  wheel_packet_init(pk, src, tgt, cidx);
+}
+// the wheels' hard points and the four wheel rays against the world (the first half of vehicle_update)
+RSX_HD RSX_NOINL inline void vehicle_rays(ArenaState& S, const StaticData& D, int ci, WheelHit hits[kWheels]) {
+  RayPacket pk;
+  vehicle_rays_begin(S, D, ci, pk);
   RSX_ZONE_BEGIN(z_rays);
-  cast_wheel_rays(S, D, src, tgt, cidx, hits);
+  grid_rays(S, D, &pk);
   RSX_ZONE_END(z_rays, 1);
+  wheel_packet_hits(S, D, pk, hits);
 }
 
 // the wheels' response to the ray hits: suspension, friction and their impulses (the second half of vehicle_update)

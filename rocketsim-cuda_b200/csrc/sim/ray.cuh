@@ -62,15 +62,20 @@ RSX_F void raybox_dirs(const RayBox& r, float o[3][4], float inv[3][4]) {
     inv[2][l] = isfinite_(c) ? c : kFltMax;
   }
 }
+// ray l's slab test against a box: the entry and exit fractions
+RSX_F void slab1(const float o[3][4], const float inv[3][4], const Box3& b, int l, float* enter, float* exit) {
+  float x0 = fmul(fsub(b.lo.x, o[0][l]), inv[0][l]), x1 = fmul(fsub(b.hi.x, o[0][l]), inv[0][l]);
+  float y0 = fmul(fsub(b.lo.y, o[1][l]), inv[1][l]), y1 = fmul(fsub(b.hi.y, o[1][l]), inv[1][l]);
+  float z0 = fmul(fsub(b.lo.z, o[2][l]), inv[2][l]), z1 = fmul(fsub(b.hi.z, o[2][l]), inv[2][l]);
+  *enter = sse_max(sse_max(sse_min(x0, x1), sse_min(y0, y1)), sse_min(z0, z1));
+  *exit = sse_min(sse_min(sse_max(x0, x1), sse_max(y0, y1)), sse_max(z0, z1));
+}
 // bit l set when ray l crosses the box within [0, lmax[l]]
 RSX_F uint32_t slab4(const float o[3][4], const float inv[3][4], const Box3& b, const float lmax[4]) {
   uint32_t m = 0;
   for (int l = 0; l < 4; ++l) {
-    float x0 = fmul(fsub(b.lo.x, o[0][l]), inv[0][l]), x1 = fmul(fsub(b.hi.x, o[0][l]), inv[0][l]);
-    float y0 = fmul(fsub(b.lo.y, o[1][l]), inv[1][l]), y1 = fmul(fsub(b.hi.y, o[1][l]), inv[1][l]);
-    float z0 = fmul(fsub(b.lo.z, o[2][l]), inv[2][l]), z1 = fmul(fsub(b.hi.z, o[2][l]), inv[2][l]);
-    float enter = sse_max(sse_max(sse_min(x0, x1), sse_min(y0, y1)), sse_min(z0, z1));
-    float exit = sse_min(sse_min(sse_max(x0, x1), sse_max(y0, y1)), sse_max(z0, z1));
+    float enter, exit;
+    slab1(o, inv, b, l, &enter, &exit);
     if (enter <= exit && exit >= 0.0f && enter <= lmax[l]) m |= 1u << l;
   }
   return m;
@@ -94,27 +99,81 @@ RSX_F void lr_hit(LocalRays* lr, V3 n_local, float frac, int r) {
 }
 
 // ---- triangle mesh through the wide BVH ----
-RSX_F void ray_triangle(LocalRays* lr, const Tri& t, float* lmax, int r) {
-  const float tol = -0.0001f;
-  float dist = dot(t.p0, t.n);
-  float da = fsub(dot(t.n, lr->from[r]), dist);
-  float db = fsub(dot(t.n, lr->to[r]), dist);
-  if (fmul(da, db) >= 0.0f) return;
-  float distance = fdiv(da, fsub(da, db));
-  float hf = lr->frac[r];
-  if (distance >= hf) {
-    *lmax = rmin(*lmax, hf);
-    return;
+// A mesh test walks the BVH with the rays' union box (internal nodes) and tests each reached leaf in walk order: the
+// leaf box's slab test against each ray's running limit lmax, then the ray-triangle test of the rays it lets through,
+// whose hits update the packet and the limits (the reference's quad_ray_shapes.cuh:377-405, quad_ray.cuh's slab test
+// and the closest-hit callback).  Each leaf is split into an evaluation that depends only on the body's local rays and
+// the fractions held when the body's test began (ray_leaf_eval: the slab's entry and exit, the triangle's crossing
+// fraction and its classification) and a replay of the decisions that depend on the running limits and hits
+// (ray_leaf_replay: the slab's limit, the callback).  Evaluating a leaf and replaying it computes what the reference's
+// leaf step computes; and since an evaluation reads nothing a replay writes, a kernel may evaluate a walk's leaves on
+// any lanes and replay them in walk order on the ray packet's owner.
+struct RayMeshJob {      // a mesh body's test: its local rays, their slab terms, the fractions when the test began
+  V3 from[4], to[4];
+  float o[3][4], inv[3][4];
+  float hf[4];
+};
+struct RayLeaf {         // one leaf's evaluation
+  float enter[4], dist[4];
+  uint32_t flags;        // bits 0-3: the slab's enter <= exit && exit >= 0; bits 4-11: per ray 0 no effect, 1 crossing at or
+                         // past the starting fraction (caps lmax), 2 a hit at dist; bits 12-15: the ray meets the back side
+};
+RSX_F void ray_mesh_job(const LocalRays& lr, const RayBox& rb, RayMeshJob& j) {
+  raybox_dirs(rb, j.o, j.inv);
+  for (int i = 0; i < 4; ++i) {
+    j.from[i] = lr.from[i];
+    j.to[i] = lr.to[i];
+    j.hf[i] = lr.frac[i];
   }
-  V3 p = lerp(lr->from[r], lr->to[r], distance);
-  V3 v0 = t.p0 - p, v1 = t.p1 - p;
-  if (dot(cross(v0, v1), t.n) < tol) return;
-  V3 v2 = t.p2 - p;
-  if (dot(cross(v1, v2), t.n) < tol) return;
-  if (dot(cross(v2, v0), t.n) < tol) return;
-  float prev = lr->pk->frac[r];
-  lr_hit_internal(lr, da <= 0.0f ? -t.n : t.n, distance, r);
-  if (lr->pk->frac[r] < prev) *lmax = lr->pk->frac[r];
+}
+// Evaluates leaf `leaf` of `mesh` for the job's rays; with lmax non-null, rays whose slab test fails at those limits
+// are not tested further (their replay skips them anyway).
+RSX_F void ray_leaf_eval(const RayMeshJob& j, const StaticData& D, const MeshInfo& mesh, uint32_t leaf, const float* lmax, RayLeaf* e) {
+  const Leaf& lf = D.leaves[mesh.leaf_first + leaf];
+  const Tri& t = D.tris[mesh.tri_first + lf.tri];
+  const float tol = -0.0001f;
+  const float dist = dot(t.p0, t.n);
+  uint32_t flags = 0;
+  for (int r = 0; r < 4; ++r) {
+    float enter, exit;
+    slab1(j.o, j.inv, lf.box, r, &enter, &exit);
+    e->enter[r] = enter;
+    e->dist[r] = 0.0f;
+    const bool ok = enter <= exit && exit >= 0.0f;
+    if (ok) flags |= 1u << r;
+    if (!ok || (lmax && !(enter <= lmax[r]))) continue;
+    float da = fsub(dot(t.n, j.from[r]), dist);
+    float db = fsub(dot(t.n, j.to[r]), dist);
+    if (fmul(da, db) >= 0.0f) continue;
+    float distance = fdiv(da, fsub(da, db));
+    e->dist[r] = distance;
+    if (distance >= j.hf[r]) {
+      flags |= 1u << (4 + 2 * r);
+      continue;
+    }
+    V3 p = lerp(j.from[r], j.to[r], distance);
+    V3 v0 = t.p0 - p, v1 = t.p1 - p;
+    if (dot(cross(v0, v1), t.n) < tol) continue;
+    V3 v2 = t.p2 - p;
+    if (dot(cross(v1, v2), t.n) < tol) continue;
+    if (dot(cross(v2, v0), t.n) < tol) continue;
+    flags |= (2u << (4 + 2 * r)) | ((da <= 0.0f ? 1u : 0u) << (12 + r));
+  }
+  e->flags = flags;
+}
+RSX_F void ray_leaf_replay(LocalRays* lr, float lmax[4], const StaticData& D, const MeshInfo& mesh, uint32_t leaf, const RayLeaf& e) {
+  for (int r = 0; r < 4; ++r) {
+    if (!((e.flags >> r) & 1u) || !(e.enter[r] <= lmax[r])) continue;
+    const uint32_t code = (e.flags >> (4 + 2 * r)) & 3u;
+    if (code == 1u) {
+      lmax[r] = rmin(lmax[r], lr->frac[r]);
+    } else if (code == 2u) {
+      const Tri& t = D.tris[mesh.tri_first + D.leaves[mesh.leaf_first + leaf].tri];
+      float prev = lr->pk->frac[r];
+      lr_hit_internal(lr, ((e.flags >> (12 + r)) & 1u) ? -t.n : t.n, e.dist[r], r);
+      if (lr->pk->frac[r] < prev) lmax[r] = lr->pk->frac[r];
+    }
+  }
 }
 RSX_F uint32_t node_mask(const WideNode& n, const Box3& b) {
   uint32_t m = 0;
@@ -125,29 +184,52 @@ RSX_F uint32_t node_mask(const WideNode& n, const Box3& b) {
   }
   return m & n.valid;
 }
-RSX_HD RSX_NOINL inline void ray_mesh(const StaticData& D, const MeshInfo& mesh, LocalRays* lr, RayBox* rb) {
-  if (!box_overlap(rb->box, mesh.root_box)) return;
-  float o[3][4], inv[3][4];
-  raybox_dirs(*rb, o, inv);
+// The leaves of a mesh body's walk, in order, across the body's meshes: resumable (one leaf per call).
+struct RayWalk {
+  int mesh;  // the mesh being walked (kMeshes: done)
+  int n;
   uint32_t stack[128];
-  stack[0] = 0;
-  int sp = 1;
-  while (sp != 0) {
-    uint32_t w = stack[--sp];
-    if (w & 0x80000000u) {
-      const Leaf& lf = D.leaves[mesh.leaf_first + (w & 0x7FFFFFFFu)];
-      uint32_t m = slab4(o, inv, lf.box, rb->lmax);
-      if (m) {
-        const Tri& t = D.tris[mesh.tri_first + lf.tri];
-        for (int i = 0; i < 4; ++i)
-          if (m & (1u << i)) ray_triangle(lr, t, &rb->lmax[i], i);
-      }
-      continue;
+};
+RSX_F void ray_walk_seek(RayWalk& w, const StaticData& D, uint32_t body, const Box3& box, int from) {
+  for (w.mesh = from; w.mesh < kMeshes; ++w.mesh)
+    if (D.meshes[w.mesh].body == body && box_overlap(box, D.meshes[w.mesh].root_box)) {
+      w.stack[0] = 0;
+      w.n = 1;
+      return;
     }
-    const WideNode& n = D.nodes[mesh.node_first + w];
-    uint32_t m = node_mask(n, rb->box);
-    for (int l = (int)n.n_child - 1; l >= 0; --l)
-      if (m & (1u << l)) stack[sp++] = n.child[l];
+  w.n = 0;
+}
+RSX_F bool ray_walk_next(RayWalk& w, const StaticData& D, uint32_t body, const Box3& box, int* mesh, uint32_t* leaf) {
+  while (w.mesh < kMeshes) {
+    const MeshInfo& m = D.meshes[w.mesh];
+    while (w.n != 0) {
+      uint32_t x = w.stack[--w.n];
+      if (x & 0x80000000u) {
+        *mesh = w.mesh;
+        *leaf = x & 0x7FFFFFFFu;
+        return true;
+      }
+      const WideNode& nd = D.nodes[m.node_first + x];
+      uint32_t mk = node_mask(nd, box);
+      for (int l = (int)nd.n_child - 1; l >= 0; --l)
+        if (mk & (1u << l)) w.stack[w.n++] = nd.child[l];
+    }
+    ray_walk_seek(w, D, body, box, w.mesh + 1);
+  }
+  return false;
+}
+// the whole test of a mesh body, leaf by leaf
+RSX_HD RSX_NOINL inline void ray_mesh_body(const StaticData& D, uint32_t body, LocalRays* lr, RayBox* rb) {
+  RayMeshJob j;
+  ray_mesh_job(*lr, *rb, j);
+  RayWalk w;
+  ray_walk_seek(w, D, body, rb->box, 0);
+  int mesh;
+  uint32_t leaf;
+  while (ray_walk_next(w, D, body, rb->box, &mesh, &leaf)) {
+    RayLeaf e;
+    ray_leaf_eval(j, D, D.meshes[mesh], leaf, rb->lmax, &e);
+    ray_leaf_replay(lr, rb->lmax, D, D.meshes[mesh], leaf, e);
   }
 }
 
@@ -383,10 +465,9 @@ RSX_F void ray_box(const BodyConst& bc, LocalRays* lr, const RayBox& rb) {
 }
 
 // ---- one candidate body (collision_world quad_ray_test) ----
-RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk) {
-  RSX_ZONE_BEGIN(z_setup);
+// the body's local rays (the packet's rays in the body's frame, their fractions so far) and their box
+RSX_F void ray_body_setup(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk, LocalRays& lr, RayBox& rb) {
   View co = view(S, D, w);
-  const BodyConst& bc = D.bodies[w];
   V3 fl[4], tl[4];
   if (m3_is_identity(co.xf.m)) {
     for (int i = 0; i < 4; ++i) {
@@ -400,7 +481,6 @@ RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, 
       tl[i] = xform_point(inv, pk->to[i]);
     }
   }
-  LocalRays lr;
   for (int i = 0; i < 4; ++i) {
     lr.from[i] = fl[i];
     lr.to[i] = tl[i];
@@ -409,9 +489,15 @@ RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, 
   lr.rot = co.xf.m;
   lr.body = w;
   lr.pk = pk;
-  RayBox rb;
   raybox_init(rb, fl, tl);
   for (int i = 0; i < 4; ++i) rb.lmax[i] = lr.frac[i];
+}
+RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, uint32_t w, RayPacket* pk) {
+  RSX_ZONE_BEGIN(z_setup);
+  const BodyConst& bc = D.bodies[w];
+  LocalRays lr;
+  RayBox rb;
+  ray_body_setup(S, D, w, pk, lr, rb);
   RSX_ZONE_END(z_setup, 28);
   RSX_ZONE_BEGIN(z_shape);
   if (bc.shape == SHAPE_BOX) {
@@ -425,8 +511,7 @@ RSX_HD RSX_NOINL inline void ray_body(const ArenaState& S, const StaticData& D, 
       if (D.planes[p].body == w) ray_plane(D.planes[p], &lr, rb);
     RSX_ZONE_END(z_shape, 26);
   } else {
-    for (int m = 0; m < kMeshes; ++m)
-      if (D.meshes[m].body == w) ray_mesh(D, D.meshes[m], &lr, &rb);
+    ray_mesh_body(D, w, &lr, &rb);
     RSX_ZONE_END(z_shape, 27);
   }
 }
@@ -444,7 +529,8 @@ RSX_F bool ray_accepts(const StaticData& D, uint32_t h, const RayPacket* pk) {
 }
 
 // the grid's candidate walk: one cell per distinct ray source, its static handles, then its dynamic ones
-RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
+// the candidate bodies of the packet, in the walk's order (nothing in the walk depends on the hits); returns their count
+RSX_F int grid_candidates(const ArenaState& S, const StaticData& D, const RayPacket* pk, uint32_t cand[kHandles]) {
   Box3 rbx;
   rbx.lo = vmin(pk->from[0], pk->to[0]);
   rbx.hi = vmax(pk->from[0], pk->to[0]);
@@ -462,9 +548,7 @@ RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
     for (int k = 0; k < nc; ++k) seen = seen || cells[k] == c;
     if (!seen) cells[nc++] = c;
   }
-  // the candidates in walk order first (nothing in the walk depends on the hits), then one body test per step, so that
-  // the lanes of a warp step through their lists together
-  uint32_t seen = 0, cand[kHandles];
+  uint32_t seen = 0;
   int nk = 0;
   for (int ci = 0; ci < nc; ++ci) {
     uint32_t cell = cells[ci];
@@ -483,6 +567,12 @@ RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
       if (box_overlap(rbx, proxy_box(S, D, h)) && ray_accepts(D, h, pk)) cand[nk++] = D.proxies[h].body;
     }
   }
+  return nk;
+}
+// the candidates first, then one body test per step, so that the lanes of a warp step through their lists together
+RSX_F void grid_rays(const ArenaState& S, const StaticData& D, RayPacket* pk) {
+  uint32_t cand[kHandles];
+  int nk = grid_candidates(S, D, pk, cand);
   for (int k = 0; k < nk; ++k) ray_body(S, D, cand[k], pk);
 }
 
@@ -492,8 +582,7 @@ struct WheelHit {
   uint32_t body;
 };
 
-RSX_F void cast_wheel_rays(const ArenaState& S, const StaticData& D, const V3* from, const V3* to, uint32_t ignore, WheelHit out[4]) {
-  RayPacket pk;
+RSX_F void wheel_packet_init(RayPacket& pk, const V3* from, const V3* to, uint32_t ignore) {
   for (int i = 0; i < 4; ++i) {
     pk.frac[i] = 1.0f;
     pk.body[i] = kNoBody;
@@ -506,7 +595,8 @@ RSX_F void cast_wheel_rays(const ArenaState& S, const StaticData& D, const V3* f
   pk.group = kFilterDefault | kFilterDropshot;
   pk.mask = kFilterAll;
   pk.min_dist2 = kWheelMinHitDist2;
-  grid_rays(S, D, &pk);
+}
+RSX_F void wheel_packet_hits(const ArenaState& S, const StaticData& D, const RayPacket& pk, WheelHit out[4]) {
   for (int i = 0; i < 4; ++i) {
     out[i].some = 0;
     out[i].point = vzero();
@@ -522,6 +612,12 @@ RSX_F void cast_wheel_rays(const ArenaState& S, const StaticData& D, const V3* f
       }
     }
   }
+}
+RSX_F void cast_wheel_rays(const ArenaState& S, const StaticData& D, const V3* from, const V3* to, uint32_t ignore, WheelHit out[4]) {
+  RayPacket pk;
+  wheel_packet_init(pk, from, to, ignore);
+  grid_rays(S, D, &pk);
+  wheel_packet_hits(S, D, pk, out);
 }
 
 }  // namespace sim

@@ -181,6 +181,8 @@ class DecisionRunner:
             if split == 9:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
                 for ticks in (4, 2):
                     out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None, "ticks": ticks})
+                # split 10: the wheel rays' mesh leaves pooled too (measured slower than split 9 on the headline mix)
+                out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": 10, "threshold": None})
             if binning and self.pred is not None:
                 for thr, labels in ((0.3, P.ALL_LABELS), (0.5, P.ALL_LABELS)):
                     out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr, "labels": labels})

@@ -113,7 +113,8 @@ def test_result_independent_of_block_order_and_queue(rsx, dev):
                 ("lock", 64, dperm, 2, 1), ("lock", 480, None, 1, 0), ("lock", 448, dperm, 148, 2),
                 ("lock", 96, None, 2, 2), ("lock", 512, dperm, 148, 3), ("lock", 64, None, 3, 3),
                 ("lock", 448, dperm, 148, 6), ("lock", 96, None, 2, 6), ("lock", 448, None, 148, 4), ("lock", 64, dperm, 2, 5),
-                ("lock", 448, dperm, 148, 7), ("lock", 448, dperm, 148, 9), ("lock", 96, None, 2, 9), ("lock", 512, None, 5, 9)]
+                ("lock", 448, dperm, 148, 7), ("lock", 448, dperm, 148, 9), ("lock", 96, None, 2, 9), ("lock", 512, None, 5, 9),
+                ("lock", 448, dperm, 148, 10), ("lock", 64, None, 3, 10)]
     for kind, block, order, grid, gran in variants:
         ds = dev.upload_states(st)
         res = dev.alloc_result(n)
