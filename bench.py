@@ -49,29 +49,27 @@ OBS_BYTES_PER_ARENA = 103 * 4 + 9 + 2 * 208 + 2 * 4
 OBS_REPS = 20
 PRESETS = [(p, q) for p in range(7) for q in range(7)]
 
-# Per decision-kernel counters of one 65,536-arena headline decision (the third from the start states), one ncu capture
-# of all variants (dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum, smsp__thread_inst_executed.sum;
-# the command is in profiles/k_sim8_lockstep_headline.md): DRAM bytes per arena-decision, warp instructions per
-# arena-tick, lanes active per warp instruction.
+# Per decision-kernel counters of one 65,536-arena headline decision from one ncu capture of all variants (the third
+# decision of each after 8 decisions of the plain launch from the start states, as `bench.py --profile-variants` runs
+# them: the contact-richer states the timed decisions see; dram__bytes_read.sum + dram__bytes_write.sum,
+# smsp__inst_executed.sum, smsp__thread_inst_executed.sum; the command is in profiles/k_sim8_lockstep_headline.md):
+# DRAM bytes per arena-decision, warp instructions per arena-tick, lanes active per warp instruction.
 _N, _T = 65536, 65536 * 8
+
+
+def _kc(rd, wr, inst, thr):
+    return {"dram_bytes_per_arena": (rd + wr) / _N, "warp_inst_per_arena_tick": inst / _T, "lanes_active": thr / inst,
+            "capture": "65,536 arenas, a headline decision after 8 (same size as the timed run)"}
+
+
 KERNEL_COUNTERS = {
-    "k_sim8_multi": {"dram_bytes_per_arena": (4383159552 + 4730361088) / _N, "warp_inst_per_arena_tick": 1348677201 / _T,
-                     "lanes_active": 11321300636 / 1348677201},
-    "k_sim8_lockstep_t448<6>": {"dram_bytes_per_arena": (5416755456 + 5473697024) / _N, "warp_inst_per_arena_tick": 1370361134 / _T,
-                                "lanes_active": 11653617617 / 1370361134},
-    "k_sim8_lockstep_t448<7>": {"dram_bytes_per_arena": (5465641728 + 5487573760) / _N, "warp_inst_per_arena_tick": 1371078365 / _T,
-                                "lanes_active": 11671523934 / 1371078365},
-    "k_sim8_lockstep_t512<6>": {"dram_bytes_per_arena": (5414247936 + 5471868160) / _N, "warp_inst_per_arena_tick": 1370835710 / _T,
-                                "lanes_active": 11667652598 / 1370835710},
-    "k_sim8_lockstep_t512<7>": {"dram_bytes_per_arena": (5456979712 + 5481598208) / _N, "warp_inst_per_arena_tick": 1371659501 / _T,
-                                "lanes_active": 11688968835 / 1371659501},
-    "k_sim8_lockstep_t448<9>": {"dram_bytes_per_arena": 11290000640 / _N, "warp_inst_per_arena_tick": 1345642323 / _T,
-                                "lanes_active": 12233723383 / 1345642323},
-    "k_sim8_lockstep_t512<9>": {"dram_bytes_per_arena": 11303093248 / _N, "warp_inst_per_arena_tick": 1347599346 / _T,
-                                "lanes_active": 12307438977 / 1347599346},
+    "k_sim8_multi": _kc(5144574208, 5044233472, 1597202788, 11031308758),
+    "k_sim8_lockstep_t448<7>": _kc(6331101440, 5841899776, 1605917385, 11345141599),
+    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),
+    "k_sim8_lockstep_t512<7>": _kc(6317576960, 5836163584, 1606528329, 11363532967),
+    "k_sim8_lockstep_t512<9>": _kc(6301496320, 5760274176, 1328764680, 11945208080),
+    "k_sim8_lockstep_t448<10>": _kc(6391429632, 5752290048, 1284026061, 11995119208),
 }
-for _k in KERNEL_COUNTERS.values():
-    _k["capture"] = "65,536 arenas, the headline decision 3 (same size as the timed run)"
 
 
 def kernel_name(config):
@@ -753,22 +751,31 @@ def large_leg(args, dev, pred, L):
 
 
 def profile_variants(args, leg):
-    """For an ncu capture at the headline size: for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 7 / 9), two decisions and then the captured one, each from the same start states."""
+    """For ncu captures at the headline size: 8 decisions of the plain launch from the start states (the states the bench
+    times are later, contact-richer ones), then for the plain launch and each lockstep variant the autotuner considers
+    (blocks 448 / 512, splits 7 / 9, and split 10 at 448), two decisions and then a third, each from those states.
+    Launch order: k_sim8_multi x 8, then 3 launches per variant in the order printed."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (7, 9)]
+                                                   for b in (448, 512) for s in (7, 9)] + \
+               [{"mode": "lockstep", "block": 448, "grid": leg.run.sms, "split": 10}]
+    run = leg.run
+    run.restore(leg.start)
+    for s in range(8):
+        run.step(leg.dctl[s % leg.steps].data_ptr(), {"mode": "plain", "block": 32})
+    warm = run.snapshot()
     out = []
     for cfg in variants:
-        leg.run.restore(leg.start)
+        run.restore(warm)
         e0, e1 = leg.torch.cuda.Event(enable_timing=True), leg.torch.cuda.Event(enable_timing=True)
         for s in range(3):
             if s == 2:
-                e0.record(leg.run.stream)
-            leg.run.step(leg.dctl[s].data_ptr(), cfg)
-        e1.record(leg.run.stream)
+                e0.record(run.stream)
+            run.step(leg.dctl[(8 + s) % leg.steps].data_ptr(), cfg)
+        e1.record(run.stream)
         e1.synchronize()
         out.append({"kernel": kernel_name(cfg), "ms": e0.elapsed_time(e1)})
-    print(json.dumps({"profile_variants": out, "arenas": leg.n}))
+    print(json.dumps({"profile_variants": out, "arenas": leg.n, "warmup_plain_decisions": 8}))
+    del warm
     leg.free()
 
 
@@ -903,7 +910,7 @@ def zones(args, dev):
             raise RuntimeError(f"zone run failed ({rc})")
         tot += out.astype(np.float64)
     if args.zones_lockstep:
-        pieces = [40, 41, 42, 43, 44, 45, 46, 47, 48, 49, 29, 30]
+        pieces = [40, 41, 42, 43, 44, 45, 46, 47, 48, 49, 29, 30, 33, 34, 35]  # 33-35: P3b's pieces in the pooled splits
         bars = [50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 31, 32]
     else:
         pieces, bars = [40 + k for k in range(10)], [50 + k for k in range(10)]
