@@ -105,9 +105,9 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=9,
+    ap.add_argument("--split", type=int, default=10,
                     help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts, "
-                         "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block")
+                         "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block, 10 = 9 + the wheel rays' mesh leaves pooled")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain launch's comparison timing")
     ap.add_argument("--no-oracle", action="store_true", help="skip the word-for-word replay through the oracle")
@@ -188,7 +188,8 @@ def oracle_compare(L, sds, idx, st0, ctl, sample, got_words, got_res, got_ev):
     smp = np.ascontiguousarray(sample.astype(np.uint32))
     sidx = np.ascontiguousarray(idx[sample])
     t = time.perf_counter()
-    L.rsref_run_batch_ex(st.ctypes.data, m, np.ascontiguousarray(sds).ctypes.data, sidx.ctypes.data, ctl.ctypes.data, ctl.shape[1],
+    sdsc = np.ascontiguousarray(sds)  # referenced until the call returns (a copy when sds is not contiguous)
+    L.rsref_run_batch_ex(st.ctypes.data, m, sdsc.ctypes.data, sidx.ctypes.data, ctl.ctypes.data, ctl.shape[1],
                          smp.ctypes.data, d, 0, res.ctypes.data, ev.ctypes.data)
     secs = time.perf_counter() - t
     bad_state = np.any(st[:, :TICK_WORDS] != got_words[:, :TICK_WORDS], axis=1)
@@ -539,7 +540,7 @@ def run_ours(args):
         Zs, Ys = [], []
         with torch.cuda.stream(run.stream):  # the copies on the stream the kernels wrote on
             for s in range(leg.steps):
-                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 9, "threshold": 0.5})
+                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 10, "threshold": 0.5})
                 Zs.append(run.Z.clone())
                 Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         run.stream.synchronize()
@@ -753,11 +754,10 @@ def large_leg(args, dev, pred, L):
 def profile_variants(args, leg):
     """For ncu captures at the headline size: 8 decisions of the plain launch from the start states (the states the bench
     times are later, contact-richer ones), then for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 7 / 9, and split 10 at 448), two decisions and then a third, each from those states.
+    (blocks 448 / 512, splits 7 / 9 / 10), two decisions and then a third, each from those states.
     Launch order: k_sim8_multi x 8, then 3 launches per variant in the order printed."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (7, 9)] + \
-               [{"mode": "lockstep", "block": 448, "grid": leg.run.sms, "split": 10}]
+                                                   for b in (448, 512) for s in (7, 9, 10)]
     run = leg.run
     run.restore(leg.start)
     for s in range(8):
@@ -801,7 +801,7 @@ def sweep(args, dev):
         t0 = time.perf_counter()
         run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
         train_s = time.perf_counter() - t0
-        base = {"block": 448, "grid": run.sms, "split": 9}
+        base = {"block": 448, "grid": run.sms, "split": 10}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
                           ("binned", {"mode": "binned", "threshold": 0.5, **base}),
@@ -836,8 +836,11 @@ def sweep(args, dev):
             m = len(sample)
             res = np.zeros((D + 1, m), np.uint32)
             ev = np.zeros((D + 1, m), np.uint32)
-            L.rsref_run_batch_ex(st0.ctypes.data, m, np.ascontiguousarray(sds).ctypes.data, np.ascontiguousarray(idx[sample]).ctypes.data,
-                                 ctl_host.ctypes.data, n, np.ascontiguousarray(sample.astype(np.uint32)).ctypes.data, D + 1, 0,
+            # every array handed to the C call by address stays referenced until the call returns
+            sdsc = np.ascontiguousarray(sds)
+            sidx = np.ascontiguousarray(idx[sample])
+            smp = np.ascontiguousarray(sample.astype(np.uint32))
+            L.rsref_run_batch_ex(st0.ctypes.data, m, sdsc.ctypes.data, sidx.ctypes.data, ctl_host.ctypes.data, n, smp.ctypes.data, D + 1, 0,
                                  res.ctypes.data, ev.ctypes.data)
             last = words["plain"][1].index_select(0, a[:, 0]).cpu().numpy().view(np.uint32)
             rec["oracle_sample"] = {"arenas": m, "decisions": D + 1,

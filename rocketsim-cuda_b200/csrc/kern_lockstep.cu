@@ -64,10 +64,11 @@ struct PoolSmem {
   uint32_t pair_tri[kPoolPairs];
   sim::LeafHit hit[kPoolPairs];
 };
-// split 10: the wheel rays' mesh leaves pooled the same way (sim/ray.cuh: evaluated anywhere, replayed on the owner)
+// split 10: the wheel rays' mesh leaves pooled too (sim/ray.cuh: evaluated anywhere, replayed on the owner)
 constexpr int kRayJobs = 64;
 constexpr int kRayPairs = 512;
-constexpr int kRayChunk = 16;
+constexpr int kRayJobsLane = 4;
+constexpr int kRayLeavesLane = 48;
 struct RayPoolSmem {
   sim::RayMeshJob job[kRayJobs];
   const StaticData* jd[kRayJobs];
@@ -186,96 +187,104 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
 }
 
 // The wheel rays of car ci of the thread's arena (act) with the mesh leaves of the whole block pooled; every thread of
-// the block calls it.  Each round, every lane runs its candidate bodies in order up to its next mesh body (planes, the
-// ball and the other car are tested in place), sets that body's test up and takes up to kRayChunk leaves of its walk;
-// all threads evaluate the published leaves; each owner replays its leaves in walk order (slab limits, hits) and moves
-// to the next candidate when the walk is done.  Results equal vehicle_rays'.
+// the block calls it.  A mesh body's walk reads only the body-local rays' box, and a leaf's evaluation made with the
+// starting fractions at 1 serves any later ones (sim/ray.cuh), so each lane first walks every mesh candidate of its
+// packet (up to kRayJobsLane bodies, kRayLeavesLane leaves), the block evaluates all those leaves at once, and each
+// owner then runs its candidates in order: mesh bodies by replaying their evaluated leaves against the fractions held
+// at that point, the plane, ball and car bodies by testing them in place.  One pool round per car; results equal
+// vehicle_rays'.  Lanes past the pool's capacity or their own budget run vehicle_rays' sequence.
 __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, bool act, int ci, sim::WheelHit hits[kWheels]) {
   Pools& u = pools();
   RayPoolSmem& sm = u.rays;
   sim::RayPacket pk;
   uint32_t cand[kHandles];
-  int nk = 0, kc = 0;
+  int nk = 0;
   if (act) {
     sim::vehicle_rays_begin(s, *D, ci, pk);
     nk = sim::grid_candidates(s, *D, &pk, cand);
   }
-  bool open = false, wdone = false;
-  sim::LocalRays lr;
-  sim::RayBox rb;
-  sim::RayWalk wk;
-  sim::RayMeshJob mj;
-  uint32_t leaves[kRayChunk];
-  int meshes[kRayChunk];
-  for (;;) {
-    int k = 0;
-    if (act) {
-      while (!open && kc < nk) {
-        const uint32_t w = cand[kc];
-        if (D->bodies[w].shape == sim::SHAPE_MESH) {
-          sim::ray_body_setup(s, *D, w, &pk, lr, rb);
-          sim::ray_mesh_job(lr, rb, mj);
-          sim::ray_walk_seek(wk, *D, w, rb.box, 0);
-          open = true;
-          wdone = false;
-        } else {
-          sim::ray_body(s, *D, w, &pk);
-          ++kc;
-        }
-      }
-      if (open) {
-        int mesh;
-        uint32_t leaf;
-        while (k < kRayChunk) {
-          if (!sim::ray_walk_next(wk, *D, cand[kc], rb.box, &mesh, &leaf)) {
-            wdone = true;
-            break;
-          }
-          leaves[k] = leaf;
-          meshes[k] = mesh;
-          ++k;
-        }
-      }
+  uint32_t leaves[kRayLeavesLane];
+  uint8_t meshes[kRayLeavesLane], jcand[kRayJobsLane], jstart[kRayJobsLane], jcount[kRayJobsLane];
+  int nj = 0, nl = 0;
+  bool fits = true;
+  for (int k = 0; k < nk && fits; ++k) {
+    const uint32_t w = cand[k];
+    const uint32_t shape = D->bodies[w].shape;
+    if (shape == sim::SHAPE_BOX || shape == sim::SHAPE_SPHERE || shape == sim::SHAPE_PLANE) continue;
+    if (nj == kRayJobsLane) {
+      fits = false;
+      break;
     }
-    if (!__syncthreads_or(open)) break;
-    uint32_t total;
-    const uint32_t ex = block_scan(k > 0 ? ((1u << 16) | (uint32_t)k) : 0u, &total, u);
-    const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
-    const bool pooled = k > 0 && slot < (uint32_t)kRayJobs && off + (uint32_t)k <= (uint32_t)kRayPairs;
-    if (pooled) {
-      sm.job[slot] = mj;
-      sm.jd[slot] = D;
-      for (int i = 0; i < k; ++i) {
-        sm.pair_job[off + i] = slot | ((uint32_t)meshes[i] << 16);
-        sm.pair_leaf[off + i] = leaves[i];
+    sim::LocalRays lr;
+    sim::RayBox rb;
+    sim::ray_body_setup(s, *D, w, &pk, lr, rb);
+    sim::RayWalk wk;
+    sim::ray_walk_seek(wk, *D, w, rb.box, 0);
+    int mesh;
+    uint32_t leaf;
+    const int first = nl;
+    while (sim::ray_walk_next(wk, *D, w, rb.box, &mesh, &leaf)) {
+      if (nl == kRayLeavesLane) {
+        fits = false;
+        break;
       }
-      atomicMax(&u.limit, off + (uint32_t)k);
+      leaves[nl] = leaf;
+      meshes[nl] = (uint8_t)mesh;
+      ++nl;
     }
-    __syncthreads();
-    const uint32_t npairs = u.limit;
-    for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
-      const uint32_t j = sm.pair_job[p] & 0xFFFFu;
-      const StaticData& Dj = *sm.jd[j];
-      sim::ray_leaf_eval(sm.job[j], Dj, Dj.meshes[sm.pair_job[p] >> 16], sm.pair_leaf[p], nullptr, &sm.out[p]);
-    }
-    __syncthreads();
-    if (open) {
-      for (int i = 0; i < k; ++i) {
-        const MeshInfo& m = D->meshes[meshes[i]];
-        sim::RayLeaf e;
-        if (pooled)
-          e = sm.out[off + i];
-        else  // past the pool's capacity: this lane evaluates its own leaves
-          sim::ray_leaf_eval(mj, *D, m, leaves[i], rb.lmax, &e);
-        sim::ray_leaf_replay(&lr, rb.lmax, *D, m, leaves[i], e);
-      }
-      if (wdone) {
-        open = false;
-        ++kc;
-      }
-    }
+    jcand[nj] = (uint8_t)k;
+    jstart[nj] = (uint8_t)first;
+    jcount[nj] = (uint8_t)(nl - first);
+    ++nj;
   }
-  if (act) sim::wheel_packet_hits(s, *D, pk, hits);
+  if (!fits) nj = nl = 0;
+  uint32_t total;
+  const uint32_t ex = block_scan(((uint32_t)nj << 16) | (uint32_t)nl, &total, u);
+  const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
+  // all of a lane's bodies or none; pooled lanes are a prefix in scan order
+  const bool pooled = nj > 0 && slot + (uint32_t)nj <= (uint32_t)kRayJobs && off + (uint32_t)nl <= (uint32_t)kRayPairs;
+  if (pooled) {
+    for (int j = 0; j < nj; ++j) {  // no body has been tested yet: the packet's fractions are all still 1
+      sim::LocalRays lr;
+      sim::RayBox rb;
+      sim::ray_body_setup(s, *D, cand[jcand[j]], &pk, lr, rb);
+      sim::ray_mesh_job(lr, rb, sm.job[slot + j]);
+      sm.jd[slot + j] = D;
+      for (int t = 0; t < jcount[j]; ++t) {
+        sm.pair_job[off + jstart[j] + t] = (slot + j) | ((uint32_t)meshes[jstart[j] + t] << 16);
+        sm.pair_leaf[off + jstart[j] + t] = leaves[jstart[j] + t];
+      }
+    }
+    atomicMax(&u.limit, off + (uint32_t)nl);
+  }
+  __syncthreads();
+  const uint32_t npairs = u.limit;
+  for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
+    const uint32_t j = sm.pair_job[p] & 0xFFFFu;
+    const StaticData& Dj = *sm.jd[j];
+    sim::ray_leaf_eval(sm.job[j], Dj, Dj.meshes[sm.pair_job[p] >> 16], sm.pair_leaf[p], nullptr, &sm.out[p]);
+  }
+  __syncthreads();
+  if (act) {
+    int j = 0;
+    for (int k = 0; k < nk; ++k) {
+      const uint32_t w = cand[k];
+      if (pooled && j < nj && jcand[j] == k) {
+        sim::LocalRays lr;
+        sim::RayBox rb;
+        sim::ray_body_setup(s, *D, w, &pk, lr, rb);
+        for (int t = 0; t < jcount[j]; ++t) {
+          const int q = jstart[j] + t;
+          sim::ray_leaf_replay(&lr, rb.lmax, *D, D->meshes[meshes[q]], leaves[q], sm.out[off + q]);
+        }
+        ++j;
+      } else {
+        sim::ray_body(s, *D, w, &pk);
+      }
+    }
+    sim::wheel_packet_hits(s, *D, pk, hits);
+  }
+  __syncthreads();  // the pool is read above: the next piece's writes come after every lane's reads
 }
 }  // namespace
 

@@ -115,8 +115,9 @@ struct RayMeshJob {      // a mesh body's test: its local rays, their slab terms
 };
 struct RayLeaf {         // one leaf's evaluation
   float enter[4], dist[4];
-  uint32_t flags;        // bits 0-3: the slab's enter <= exit && exit >= 0; bits 4-11: per ray 0 no effect, 1 crossing at or
-                         // past the starting fraction (caps lmax), 2 a hit at dist; bits 12-15: the ray meets the back side
+  uint32_t flags;        // bits 0-3: the slab's enter <= exit && exit >= 0; bits 4-7: the ray crosses the triangle's plane
+                         // (dist is the crossing fraction); bits 8-11: the crossing is inside the triangle (evaluated only
+                         // when dist is below the evaluation's starting fraction); bits 12-15: the ray meets the back side
 };
 RSX_F void ray_mesh_job(const LocalRays& lr, const RayBox& rb, RayMeshJob& j) {
   raybox_dirs(rb, j.o, j.inv);
@@ -127,7 +128,9 @@ RSX_F void ray_mesh_job(const LocalRays& lr, const RayBox& rb, RayMeshJob& j) {
   }
 }
 // Evaluates leaf `leaf` of `mesh` for the job's rays; with lmax non-null, rays whose slab test fails at those limits
-// are not tested further (their replay skips them anyway).
+// are not tested further (their replay skips them anyway).  The inside test runs for crossings below the job's
+// starting fractions hf; an evaluation made with hf = 1 therefore serves any later starting fraction (fractions only
+// fall from 1).
 RSX_F void ray_leaf_eval(const RayMeshJob& j, const StaticData& D, const MeshInfo& mesh, uint32_t leaf, const float* lmax, RayLeaf* e) {
   const Leaf& lf = D.leaves[mesh.leaf_first + leaf];
   const Tri& t = D.tris[mesh.tri_first + lf.tri];
@@ -147,32 +150,34 @@ RSX_F void ray_leaf_eval(const RayMeshJob& j, const StaticData& D, const MeshInf
     if (fmul(da, db) >= 0.0f) continue;
     float distance = fdiv(da, fsub(da, db));
     e->dist[r] = distance;
-    if (distance >= j.hf[r]) {
-      flags |= 1u << (4 + 2 * r);
-      continue;
-    }
+    flags |= (1u << (4 + r)) | ((da <= 0.0f ? 1u : 0u) << (12 + r));
+    if (distance >= j.hf[r]) continue;
     V3 p = lerp(j.from[r], j.to[r], distance);
     V3 v0 = t.p0 - p, v1 = t.p1 - p;
     if (dot(cross(v0, v1), t.n) < tol) continue;
     V3 v2 = t.p2 - p;
     if (dot(cross(v1, v2), t.n) < tol) continue;
     if (dot(cross(v2, v0), t.n) < tol) continue;
-    flags |= (2u << (4 + 2 * r)) | ((da <= 0.0f ? 1u : 0u) << (12 + r));
+    flags |= 1u << (8 + r);
   }
   e->flags = flags;
 }
+// The ray-triangle callback's decisions for one evaluated leaf, against the running limits and the fractions the body's
+// test began with (lr->frac): a crossing at or past that fraction caps the limit, one before it that lies inside the
+// triangle is a hit candidate.
 RSX_F void ray_leaf_replay(LocalRays* lr, float lmax[4], const StaticData& D, const MeshInfo& mesh, uint32_t leaf, const RayLeaf& e) {
   for (int r = 0; r < 4; ++r) {
     if (!((e.flags >> r) & 1u) || !(e.enter[r] <= lmax[r])) continue;
-    const uint32_t code = (e.flags >> (4 + 2 * r)) & 3u;
-    if (code == 1u) {
+    if (!((e.flags >> (4 + r)) & 1u)) continue;
+    if (e.dist[r] >= lr->frac[r]) {
       lmax[r] = rmin(lmax[r], lr->frac[r]);
-    } else if (code == 2u) {
-      const Tri& t = D.tris[mesh.tri_first + D.leaves[mesh.leaf_first + leaf].tri];
-      float prev = lr->pk->frac[r];
-      lr_hit_internal(lr, ((e.flags >> (12 + r)) & 1u) ? -t.n : t.n, e.dist[r], r);
-      if (lr->pk->frac[r] < prev) lmax[r] = lr->pk->frac[r];
+      continue;
     }
+    if (!((e.flags >> (8 + r)) & 1u)) continue;
+    const Tri& t = D.tris[mesh.tri_first + D.leaves[mesh.leaf_first + leaf].tri];
+    float prev = lr->pk->frac[r];
+    lr_hit_internal(lr, ((e.flags >> (12 + r)) & 1u) ? -t.n : t.n, e.dist[r], r);
+    if (lr->pk->frac[r] < prev) lmax[r] = lr->pk->frac[r];
   }
 }
 RSX_F uint32_t node_mask(const WideNode& n, const Box3& b) {
