@@ -68,7 +68,8 @@ KERNEL_COUNTERS = {
     "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),
     "k_sim8_lockstep_t512<7>": _kc(6317576960, 5836163584, 1606528329, 11363532967),
     "k_sim8_lockstep_t512<9>": _kc(6301496320, 5760274176, 1328764680, 11945208080),
-    "k_sim8_lockstep_t448<10>": _kc(6391429632, 5752290048, 1284026061, 11995119208),
+    "k_sim8_lockstep_t448<10>": _kc(6189615104, 5601586432, 1279091584, 11861312127),
+    "k_sim8_lockstep_t512<10>": _kc(6207429120, 5609150464, 1281057339, 11934370506),
 }
 
 
