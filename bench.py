@@ -126,6 +126,11 @@ def parse():
     ap.add_argument("--zones-lockstep", action="store_true", help="with --zones: the pieces of the lockstep kernel at --split (block 448)")
     ap.add_argument("--zones-skip", type=int, default=0, help="with --zones: plain decisions run first (untimed)")
     ap.add_argument("--mix", default="headline", choices=["headline", "contact"])
+    ap.add_argument("--rollout", action="store_true",
+                    help="the on-device rollout (1,048,576 arenas, contact-heavy mix, 1,000 decisions, retraining, resets) with "
+                         "a 1%% sample checked against the oracle at decisions 1, 500 and 1,000")
+    ap.add_argument("--rollout-arenas", type=int, default=1048576)
+    ap.add_argument("--rollout-decisions", type=int, default=1000)
     ap.add_argument("--profile-variants", action="store_true",
                     help="one decision of the plain launch and of each lockstep variant after two of its own, for an ncu capture")
     return ap.parse_args()
@@ -476,6 +481,8 @@ def run_ours(args):
         return sweep(args, dev)
     if args.zones:
         return zones(args, dev)
+    if args.rollout:
+        return rollout_check(args, dev)
     n = args.arenas
     sds, idx, st = world(rsx, n, rank, args.seed)
     leg = Leg(args, dev, sds, idx, st, args.seed * 1000 + rank, dist)
@@ -852,6 +859,77 @@ def sweep(args, dev):
         run.free()
         del run
         torch.cuda.empty_cache()
+
+
+def rollout_check(args, dev):
+    """The on-device rollout of rollout.py (contact-heavy mix, the learned 16-level order retrained every 64 decisions,
+    goal-ended episodes restarted on the device) with a seeded 1% sample of its arenas gathered on the device at
+    decisions 1, D / 2 and D, and replayed through the oracle decision by decision (the same controls; the same restarts,
+    from the host twin of the device's start-state generator), compared word for word.  One JSON line."""
+    import torch
+    import rsx
+    import rollout
+    from runner import DecisionRunner
+
+    n, D, K = args.rollout_arenas, args.rollout_decisions, 16
+    mix = rsx.MIX_CONTACT_HEAVY
+    sds, idx, st = world(rsx, n, 0, args.seed, mix)
+    run = DecisionRunner(dev, sds, idx, st)
+    sample = np.sort(np.random.default_rng(args.seed + 4).choice(n, max(1, n // 100), replace=False))
+    st0 = np.ascontiguousarray(st[sample])  # the sample's start states (the rest is on the device)
+    del st
+    host_pool = [rsx.decision_controls(args.seed * 1000, k, n) for k in range(K)]
+    pool = [torch.from_numpy(c.view(np.int32)).to(dev.device) for c in host_pool]
+    t0 = time.perf_counter()
+    run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
+    train_s = time.perf_counter() - t0
+    a = torch.from_numpy(sample.astype(np.int64)).to(dev.device)[:, None]
+    w = torch.arange(TICK_WORDS, device=dev.device, dtype=torch.int64)[None, :]
+    pos = ((a // 32) * (32 * rsx.ARENA_WORDS) + w * 32 + (a % 32)).reshape(-1)
+    checks = sorted({1, max(1, D // 2), D})
+    got = {}
+
+    def on_decision(d):  # after decision d and its restarts
+        if d + 1 in checks:
+            snap = run.snapshot()
+            got[d + 1] = snap[pos].reshape(len(sample), TICK_WORDS).cpu().numpy().view(np.uint32)
+            del snap
+
+    cfg = {"mode": "levels", "block": 448, "grid": run.sms, "split": args.split, "threshold": None, "levels": 16, "weights": [1.0] * 6}
+    reset_seed = args.seed * 7919
+    ro = rollout.Rollout(run, pool, reset_seed=reset_seed, mix=mix, config=cfg)
+    windows = ro.run_decisions(D, 64, on_decision=on_decision)
+    total_ms = sum(x["ms_per_decision"] * (x["decisions"][1] - x["decisions"][0] + 1) for x in windows)
+    run.free()
+    # the oracle's replay of the sample
+    L = oracle_batch()
+    check = None
+    if L is not None and hasattr(L, "rsref_run_batch_ex"):
+        t1 = time.perf_counter()
+        m = len(sample)
+        ref = st0
+        sdsc = np.ascontiguousarray(sds)
+        sidx = np.ascontiguousarray(idx[sample])
+        smp = np.ascontiguousarray(sample.astype(np.uint32))
+        res = np.zeros((1, m), np.uint32)
+        ev = np.zeros((1, m), np.uint32)
+        bad, resets = {}, 0
+        for d in range(D):
+            ctl = host_pool[d % K]
+            L.rsref_run_batch_ex(ref.ctypes.data, m, sdsc.ctypes.data, sidx.ctypes.data, ctl.ctypes.data, n, smp.ctypes.data, 1, 0,
+                                 res.ctypes.data, ev.ctypes.data)
+            hit = np.nonzero(res[0] & 0xFF)[0]
+            if hit.size:
+                resets += hit.size
+                ref[hit] = rsx.make_states_at(sds, idx[sample[hit]], sample[hit], reset_seed + d, mix)
+            if d + 1 in checks:
+                bad[d + 1] = int(np.any(got[d + 1] != ref[:, :TICK_WORDS], axis=1).sum())
+        check = {"arenas": int(m), "at_decisions": checks, "mismatches": bad, "restarts_in_sample": resets,
+                 "oracle_seconds": round(time.perf_counter() - t1, 1)}
+    print(json.dumps({"rollout": {"arenas": n, "decisions": D, "mix": "contact-heavy", "config": kernel_name(cfg) + " levels",
+                                  "initial_train_s": round(train_s, 2), "arena_ticks_per_s": n * 8 * D / (total_ms / 1e3),
+                                  "windows": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in x.items()} for x in windows]},
+                      "bit_exact_vs_oracle": check}))
 
 
 ZONE_NAMES = {0: "P1 car pre-tick head", 1: "P1 wheel rays", 2: "P1 wheel response", 3: "P1 car pre-tick tail", 10: "P3b pair heads",
