@@ -959,14 +959,19 @@ def zones(args, dev):
     import torch
     import rsx
 
-    lib = "librsx_zones_ls.so" if args.zones_lockstep else ("librsx_zones_all.so" if args.zones_all else "librsx_zones.so")
+    if args.zones_lockstep:
+        lib = "librsx_zones_ls_all.so" if args.zones_all else "librsx_zones_ls.so"
+    else:
+        lib = "librsx_zones_all.so" if args.zones_all else "librsx_zones.so"
     Z = ctypes.CDLL(os.path.join(ROOT, "rocketsim-cuda_b200", lib))
     vp = ctypes.c_void_p
     if args.zones_lockstep:
         Z.rsx_zones_lockstep.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_int, vp]
     else:
         Z.rsx_zones_decision.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp]
-    names = LOCKSTEP_ZONE_NAMES if args.zones_lockstep else ZONE_NAMES
+    names = dict(LOCKSTEP_ZONE_NAMES) if args.zones_lockstep else ZONE_NAMES
+    if args.zones_lockstep and args.zones_all:  # the simulator's own markers too (they inflate the pieces that hold them)
+        names.update({i: "    " + nm.strip() for i, nm in ZONE_NAMES.items() if i < 29})
     n = args.arenas
     sds, idx, st = world(rsx, n, 0, args.seed, rsx.MIX_HEADLINE if args.mix == "headline" else rsx.MIX_CONTACT_HEAVY)
     dsd = dev.upload_static(sds)
