@@ -63,13 +63,15 @@ def _kc(rd, wr, inst, thr):
 
 
 KERNEL_COUNTERS = {
-    "k_sim8_multi": _kc(5144574208, 5044233472, 1597202788, 11031308758),
-    "k_sim8_lockstep_t448<7>": _kc(6331101440, 5841899776, 1605917385, 11345141599),
-    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),
-    "k_sim8_lockstep_t512<7>": _kc(6317576960, 5836163584, 1606528329, 11363532967),
+    "k_sim8_multi": _kc(5166058496, 5058733568, 1597558738, 11031926045),
+    "k_sim8_lockstep_t448<7>": _kc(6338036224, 5847074304, 1607469833, 11344977176),
+    "k_sim8_lockstep_t512<7>": _kc(6336640000, 5842823424, 1608080777, 11363368544),
+    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),  # an earlier capture, same command with splits 7 / 9
     "k_sim8_lockstep_t512<9>": _kc(6301496320, 5760274176, 1328764680, 11945208080),
-    "k_sim8_lockstep_t448<10>": _kc(6189615104, 5601586432, 1279091584, 11861312127),
-    "k_sim8_lockstep_t512<10>": _kc(6207429120, 5609150464, 1281057339, 11934370506),
+    "k_sim8_lockstep_t448<10>": _kc(6185998080, 5599560448, 1278761564, 11862062842),
+    "k_sim8_lockstep_t512<10>": _kc(6201578752, 5612222720, 1282169297, 11947769025),
+    "k_sim8_lockstep_t448<11>": _kc(6159845376, 5599038976, 1279900801, 11828416481),
+    "k_sim8_lockstep_t512<11>": _kc(6171914496, 5606226432, 1282304739, 11906919556),
 }
 
 
@@ -106,7 +108,7 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=10,
+    ap.add_argument("--split", type=int, default=11,
                     help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts, "
                          "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block, 10 = 9 + the wheel rays' mesh leaves pooled")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
@@ -548,7 +550,7 @@ def run_ours(args):
         Zs, Ys = [], []
         with torch.cuda.stream(run.stream):  # the copies on the stream the kernels wrote on
             for s in range(leg.steps):
-                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 10, "threshold": 0.5})
+                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 11, "threshold": 0.5})
                 Zs.append(run.Z.clone())
                 Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         run.stream.synchronize()
@@ -762,10 +764,10 @@ def large_leg(args, dev, pred, L):
 def profile_variants(args, leg):
     """For ncu captures at the headline size: 8 decisions of the plain launch from the start states (the states the bench
     times are later, contact-richer ones), then for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 7 / 9 / 10), two decisions and then a third, each from those states.
+    (blocks 448 / 512, splits 7 / 10 / 11), two decisions and then a third, each from those states.
     Launch order: k_sim8_multi x 8, then 3 launches per variant in the order printed."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (7, 9, 10)]
+                                                   for b in (448, 512) for s in (7, 10, 11)]
     run = leg.run
     run.restore(leg.start)
     for s in range(8):
@@ -809,7 +811,7 @@ def sweep(args, dev):
         t0 = time.perf_counter()
         run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
         train_s = time.perf_counter() - t0
-        base = {"block": 448, "grid": run.sms, "split": 10}
+        base = {"block": 448, "grid": run.sms, "split": 11}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
                           ("binned", {"mode": "binned", "threshold": 0.5, **base}),
@@ -944,7 +946,7 @@ for _k, _nm in enumerate(["P0", "P1", "P2", "P3a", "P3b", "P4", "P5", "P6", "P7"
 
 
 LOCKSTEP_ZONE_NAMES = {40: "P0", 41: "P1 pre-tick head (per car)", 42: "P1 wheel rays (per car)", 43: "P1 wheel response (per car)",
-                       44: "P2", 45: "P3a (per body)", 46: "P3b", 47: "P4", 48: "P5 (3 pieces)", 49: "P6", 29: "P7", 30: "P8 (2 pieces)",
+                       44: "P2", 45: "P3a", 46: "P3b", 47: "P4", 48: "P5 (3 pieces)", 49: "P6", 29: "P7", 30: "P8 (2 pieces)",
                        33: "  P3b heads and walks", 34: "  P3b pooled leaf tests", 35: "  P3b additions and tails",
                        60: "copy-in (load_tick)", 61: "copy-out (store_tick)"}
 for _i, _nm in zip([50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 31, 32],

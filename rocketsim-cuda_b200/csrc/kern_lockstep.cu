@@ -10,7 +10,8 @@
 // loop; split 6: split 2 with P5 as rows / iterations / integration and P8 as cars / the rest; split 7: split 6 with
 // P3a one dynamic body at a time; splits 4 and 5 leave
 // the barriers out between P3b (4) or P4 (5) and P8, to measure what they buy), so that at any time the block's warps
-// fetch from one piece of code.
+// fetch from one piece of code.  Splits 9 and 10 add the pooled contact work below; split 11 is split 10 with P3a in
+// one piece again (once P3b and the rays were pooled, P3a's per-body barriers cost more than they kept together).
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         const int zp = k <= 7 ? 42 + k : 21 + k, zb = zp + (k <= 7 ? 10 : 2);
         (void)zp;
         (void)zb;
-        if (SPLIT >= 7 && k == 3) {  // P3a: one dynamic body at a time
+        if (SPLIT >= 7 && SPLIT < 11 && k == 3) {  // P3a: one dynamic body at a time (from split 11: one piece)
 #pragma unroll 1
           for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
             {
@@ -535,6 +536,7 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
   const Controls* C = (const Controls*)controls;
 #define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
   switch (split) {
+    case 11: RSX_LS_LAUNCH(11); break;
     case 10: RSX_LS_LAUNCH(10); break;
     case 9: RSX_LS_LAUNCH(9); break;
     case 8: RSX_LS_LAUNCH(8); break;
