@@ -63,15 +63,18 @@ def _kc(rd, wr, inst, thr):
 
 
 KERNEL_COUNTERS = {
-    "k_sim8_multi": _kc(5166058496, 5058733568, 1597558738, 11031926045),
-    "k_sim8_lockstep_t448<7>": _kc(6338036224, 5847074304, 1607469833, 11344977176),
-    "k_sim8_lockstep_t512<7>": _kc(6336640000, 5842823424, 1608080777, 11363368544),
-    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),  # an earlier capture, same command with splits 7 / 9
+    "k_sim8_multi": _kc(5205353728, 5090545920, 1597558738, 11031926045),
+    "k_sim8_lockstep_t448<7>": _kc(6368841216, 5860134400, 1615365164, 11353667488),
+    "k_sim8_lockstep_t512<7>": _kc(6355182592, 5853101056, 1615976108, 11372058856),
+    # splits 9 and 10: earlier captures by the same command with splits 7 / 9 / 10 and 7 / 10 / 11
+    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),
     "k_sim8_lockstep_t512<9>": _kc(6301496320, 5760274176, 1328764680, 11945208080),
     "k_sim8_lockstep_t448<10>": _kc(6185998080, 5599560448, 1278761564, 11862062842),
     "k_sim8_lockstep_t512<10>": _kc(6201578752, 5612222720, 1282169297, 11947769025),
-    "k_sim8_lockstep_t448<11>": _kc(6159845376, 5599038976, 1279900801, 11828416481),
-    "k_sim8_lockstep_t512<11>": _kc(6171914496, 5606226432, 1282304739, 11906919556),
+    "k_sim8_lockstep_t448<11>": _kc(6157746944, 5597323520, 1282829151, 11837348584),
+    "k_sim8_lockstep_t512<11>": _kc(6169138688, 5604822272, 1285928337, 11917567873),
+    "k_sim8_lockstep_t448<14>": _kc(5935916544, 5489462528, 1265547388, 12022290088),
+    "k_sim8_lockstep_t512<14>": _kc(5970577152, 5512242688, 1268913540, 12112352477),
 }
 
 
@@ -108,7 +111,7 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=11,
+    ap.add_argument("--split", type=int, default=14,
                     help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts, "
                          "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block, 10 = 9 + the wheel rays' mesh leaves pooled")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
@@ -550,7 +553,7 @@ def run_ours(args):
         Zs, Ys = [], []
         with torch.cuda.stream(run.stream):  # the copies on the stream the kernels wrote on
             for s in range(leg.steps):
-                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 11, "threshold": 0.5})
+                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 14, "threshold": 0.5})
                 Zs.append(run.Z.clone())
                 Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         run.stream.synchronize()
@@ -764,10 +767,10 @@ def large_leg(args, dev, pred, L):
 def profile_variants(args, leg):
     """For ncu captures at the headline size: 8 decisions of the plain launch from the start states (the states the bench
     times are later, contact-richer ones), then for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 7 / 10 / 11), two decisions and then a third, each from those states.
+    (blocks 448 / 512, splits 7 / 11 / 14), two decisions and then a third, each from those states.
     Launch order: k_sim8_multi x 8, then 3 launches per variant in the order printed."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (7, 10, 11)]
+                                                   for b in (448, 512) for s in (7, 11, 14)]
     run = leg.run
     run.restore(leg.start)
     for s in range(8):
@@ -811,7 +814,7 @@ def sweep(args, dev):
         t0 = time.perf_counter()
         run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
         train_s = time.perf_counter() - t0
-        base = {"block": 448, "grid": run.sms, "split": 11}
+        base = {"block": 448, "grid": run.sms, "split": 14}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
                           ("binned", {"mode": "binned", "threshold": 0.5, **base}),
@@ -935,7 +938,8 @@ def rollout_check(args, dev):
 
 
 ZONE_NAMES = {0: "P1 car pre-tick head", 1: "P1 wheel rays", 2: "P1 wheel response", 3: "P1 car pre-tick tail", 10: "P3b pair heads",
-              11: "P3b box-triangle SAT", 12: "P3b box BVH step", 13: "P3b box job tail", 14: "P3b sphere BVH step",
+              4: "  SAT: feature pairs (enumerate + first min)", 5: "  rays: candidates and mesh walks", 6: "  rays: pooled leaf evaluations",
+              7: "  rays: replays and hits", 8: "  rays: pool barriers (incl. the prefix sum)", 11: "P3b box-triangle SAT", 12: "P3b box BVH step", 13: "P3b box job tail", 14: "P3b sphere BVH step",
               15: "P3b sphere-triangle", 16: "P3b sphere job tail", 17: "  head: convex-plane", 18: "  head: sphere-box",
               19: "  head: box-box", 21: "  head: sphere job begin", 22: "  head: box job begin", 23: "  head: near tail",
               24: "  ray: box", 25: "  ray: sphere", 26: "  ray: plane", 27: "  ray: mesh", 28: "  ray: body setup",

@@ -118,8 +118,9 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
  * split 6 with P3a one dynamic body at a time; split 9 is split 7 with P3b's mesh-leaf tests pooled over the block (each
  * round every arena's next BVH leaves are tested by all threads; the owners add the hits in walk order); split 10 is
  * split 9 with the wheel rays' mesh leaves pooled too (per car, every mesh candidate's leaves evaluated by all threads
- * in one round, the owners replaying them in candidate and walk order); split 11 is split 10 with P3a in one piece (the
- * default: the fastest measured).  Register budget by block: up to 448 threads 144 registers, 512 128.  At
+ * in one round, the owners replaying them in candidate and walk order); split 11 is split 10 with P3a in one piece;
+ * split 14 is split 11 with the 47 feature pairs of the box-triangle SATs that reach them computed by the whole block
+ * (up to 18 SATs per round; the default: the fastest measured).  Register budget by block: up to 448 threads 144 registers, 512 128.  At
  * most 2^24 arenas and grid 65,535 per call.  Results equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
 #define RSX_LOCKSTEP_MAX_BLOCK 512u
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,

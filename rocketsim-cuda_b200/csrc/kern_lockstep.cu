@@ -11,7 +11,8 @@
 // P3a one dynamic body at a time; splits 4 and 5 leave
 // the barriers out between P3b (4) or P4 (5) and P8, to measure what they buy), so that at any time the block's warps
 // fetch from one piece of code.  Splits 9 and 10 add the pooled contact work below; split 11 is split 10 with P3a in
-// one piece again (once P3b and the rays were pooled, P3a's per-body barriers cost more than they kept together).
+// one piece again (once P3b and the rays were pooled, P3a's per-body barriers cost more than they kept together);
+// split 14 is split 11 with the box-triangle SATs' feature pairs computed by the whole block.
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -58,13 +59,27 @@ namespace {
 // separation is exact (sim/narrow.cuh, P3b driver).
 constexpr int kPoolJobs = 128;
 constexpr int kPoolPairs = 512;
+// split 14: up to kDeferSat box-triangle SATs of a round that reach their 47 feature pairs have those pairs computed by
+// the whole block (stage B) before their owners' threads finish them (stage C); the pairs overlay the job records, which
+// no thread reads after the first stage of the tests.
+constexpr int kDeferSat = 18;
 struct PoolSmem {
-  sim::LeafJob job[kPoolJobs];
-  const StaticData* jd[kPoolJobs];
-  uint32_t pair_job[kPoolPairs];
-  uint32_t pair_tri[kPoolPairs];
+  union {
+    struct {
+      sim::LeafJob job[kPoolJobs];
+      const StaticData* jd[kPoolJobs];
+      uint32_t pair_job[kPoolPairs];
+      uint32_t pair_tri[kPoolPairs];
+    };
+    sim::FeatPair feat[kDeferSat][sim::kPairs];
+  };
   sim::LeafHit hit[kPoolPairs];
+  sim::SatFront front[kDeferSat];
+  uint32_t front_pair[kDeferSat];
 };
+static_assert(sizeof(sim::FeatPair) * kDeferSat * sim::kPairs <=
+                  sizeof(sim::LeafJob) * kPoolJobs + sizeof(void*) * kPoolJobs + sizeof(uint32_t) * 2 * kPoolPairs,
+              "the feature pairs fit over the job records");
 // split 10: the wheel rays' mesh leaves pooled too (sim/ray.cuh: evaluated anywhere, replayed on the owner)
 constexpr int kRayJobs = 64;
 constexpr int kRayPairs = 512;
@@ -85,6 +100,7 @@ struct Pools {
   };
   uint32_t warp_sum[32];
   uint32_t limit;
+  uint32_t deferred;  // split 14: SATs of this round whose feature pairs the block computes
 };
 __device__ __forceinline__ Pools& pools() {
   __shared__ Pools u;
@@ -101,7 +117,10 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, Pool
     if (lane >= (uint32_t)d) x += y;
   }
   if (lane == 31) sm.warp_sum[warp] = x;
-  if (threadIdx.x == 0) sm.limit = 0;
+  if (threadIdx.x == 0) {
+    sm.limit = 0;
+    sm.deferred = 0;
+  }
   __syncthreads();
   if (warp == 0) {
     uint32_t w = lane < nw ? sm.warp_sum[lane] : 0u;
@@ -117,7 +136,9 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* total, Pool
   return (warp ? sm.warp_sum[warp - 1] : 0u) + x - v;
 }
 
-// P3b of the thread's arena (have) with pooled leaf tests; every thread of the block calls it
+// P3b of the thread's arena (have) with pooled leaf tests; every thread of the block calls it.  SplitSat (split 14): the
+// box-triangle SATs that reach their feature pairs have them computed by the whole block.
+template <bool SplitSat>
 __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool have, int* un) {
   Pools& u = pools();
   PoolSmem& sm = u.p3b;
@@ -164,11 +185,46 @@ __device__ __noinline__ void p3b_pooled(ArenaState& s, const StaticData* D, bool
     for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
       const uint32_t j = sm.pair_job[p];
       sim::LeafHit h;
-      sim::leaf_test(sm.job[j], *sm.jd[j], sm.pair_tri[p], &h);
+      if (!SplitSat) {
+        sim::leaf_test(sm.job[j], *sm.jd[j], sm.pair_tri[p], &h);
+      } else {
+        sim::SatFront f;
+        if (!sim::leaf_test_front(sm.job[j], *sm.jd[j], sm.pair_tri[p], &h, &f)) {
+          const uint32_t d = atomicAdd(&u.deferred, 1u);
+          if (d < (uint32_t)kDeferSat) {  // the block computes its feature pairs below
+            sm.front[d] = f;
+            sm.front_pair[d] = p;
+            continue;
+          }
+          sim::FeatPair P[sim::kPairs];  // past the deferred capacity: this thread computes them itself
+          sim::enum_pairs(f.hu, f.q, f.e, P);
+          sim::leaf_test_back(f, P, &h);
+        }
+      }
       sm.hit[p] = h;
     }
     RSX_ZONE_END(zt, 34);
     LS_SYNC(56);
+    if (SplitSat) {
+      const uint32_t nd = min(u.deferred, (uint32_t)kDeferSat);
+      if (nd != 0) {  // (uniform: every thread read the count after the barrier)
+        RSX_ZONE_BEGIN(zf);
+        for (uint32_t w = threadIdx.x; w < nd * (uint32_t)sim::kPairs; w += blockDim.x) {
+          const uint32_t d = w / (uint32_t)sim::kPairs, i = w % (uint32_t)sim::kPairs;
+          sm.feat[d][i] = sim::feat_pair(sm.front[d], (int)i);
+        }
+        RSX_ZONE_END(zf, 34);
+        LS_SYNC(56);
+        RSX_ZONE_BEGIN(zg);
+        for (uint32_t d = threadIdx.x; d < nd; d += blockDim.x) {
+          sim::LeafHit h;
+          sim::leaf_test_back(sm.front[d], sm.feat[d], &h);
+          sm.hit[sm.front_pair[d]] = h;
+        }
+        RSX_ZONE_END(zg, 34);
+        LS_SYNC(56);
+      }
+    }
     RSX_ZONE_BEGIN(zc);
     if (pooled) {
       for (int i = 0; i < k; ++i)
@@ -200,6 +256,7 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
   sim::RayPacket pk;
   uint32_t cand[kHandles];
   int nk = 0;
+  RSX_ZONE_BEGIN(zr0);
   if (act) {
     sim::vehicle_rays_begin(s, *D, ci, pk);
     nk = sim::grid_candidates(s, *D, &pk, cand);
@@ -239,6 +296,8 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
     ++nj;
   }
   if (!fits) nj = nl = 0;
+  RSX_ZONE_END(zr0, 5);
+  RSX_ZONE_BEGIN(zr1);
   uint32_t total;
   const uint32_t ex = block_scan(((uint32_t)nj << 16) | (uint32_t)nl, &total, u);
   const uint32_t slot = ex >> 16, off = ex & 0xFFFFu;
@@ -259,13 +318,19 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
     atomicMax(&u.limit, off + (uint32_t)nl);
   }
   __syncthreads();
+  RSX_ZONE_END(zr1, 8);
+  RSX_ZONE_BEGIN(zr2);
   const uint32_t npairs = u.limit;
   for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
     const uint32_t j = sm.pair_job[p] & 0xFFFFu;
     const StaticData& Dj = *sm.jd[j];
     sim::ray_leaf_eval(sm.job[j], Dj, Dj.meshes[sm.pair_job[p] >> 16], sm.pair_leaf[p], nullptr, &sm.out[p]);
   }
+  RSX_ZONE_END(zr2, 6);
+  RSX_ZONE_BEGIN(zr3);
   __syncthreads();
+  RSX_ZONE_END(zr3, 8);
+  RSX_ZONE_BEGIN(zr4);
   if (act) {
     int j = 0;
     for (int k = 0; k < nk; ++k) {
@@ -285,7 +350,10 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
     }
     sim::wheel_packet_hits(s, *D, pk, hits);
   }
-  __syncthreads();  // the pool is read above: the next piece's writes come after every lane's reads
+  RSX_ZONE_END(zr4, 7);
+  RSX_ZONE_BEGIN(zr5);
+  __syncthreads();
+  RSX_ZONE_END(zr5, 8);  // the pool is read above: the next piece's writes come after every lane's reads
 }
 }  // namespace
 
@@ -452,7 +520,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           continue;
         }
         if (SPLIT >= 9 && k == 4) {  // P3b with the block's leaf tests pooled
-          p3b_pooled(s, D, have, &un);
+          p3b_pooled<SPLIT == 14>(s, D, have, &un);
           continue;
         }
         if (SPLIT == 3 && k == 4) {
@@ -536,6 +604,7 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
   const Controls* C = (const Controls*)controls;
 #define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
   switch (split) {
+    case 14: RSX_LS_LAUNCH(14); break;
     case 11: RSX_LS_LAUNCH(11); break;
     case 10: RSX_LS_LAUNCH(10); break;
     case 9: RSX_LS_LAUNCH(9); break;

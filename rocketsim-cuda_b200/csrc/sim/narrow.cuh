@@ -1109,6 +1109,29 @@ RSX_F bool leaf_test(const LeafJob& j, const StaticData& D, uint32_t tri, LeafHi
   RSX_ZONE_END(z_stri, 15);
   return f;
 }
+// leaf_test in stages, for callers that share a box-triangle SAT's feature pairs among threads: true when the test is
+// complete (h set); false when the SAT goes on from f (feat_pair, then leaf_test_back).  Same results as leaf_test.
+RSX_F bool leaf_test_front(const LeafJob& j, const StaticData& D, uint32_t tri, LeafHit* h, SatFront* f) {
+  if (j.kind != NEAR_BOX_JOB) {  // a sphere-triangle test is always complete (leaf_test's value is whether it found one)
+    leaf_test(j, D, tri, h);
+    return true;
+  }
+  const Tri& t = D.tris[j.tri_first + tri];
+  V3 q[3] = {xform_point(j.mesh_to_box, t.p0), xform_point(j.mesh_to_box, t.p1), xform_point(j.mesh_to_box, t.p2)};
+  SatHit sh;
+  const int r = sat_front(j.box_xf, j.half, j.margin, q, j.maxd, &sh, f);
+  if (r == SAT_PAIRS) return false;
+  h->found = r == SAT_HIT;
+  h->point = sh.point_world;
+  h->depth = sh.distance;
+  return true;
+}
+RSX_F void leaf_test_back(const SatFront& f, const FeatPair* P, LeafHit* h) {
+  SatHit sh;
+  h->found = sat_back(f, P, &sh);
+  h->point = sh.point_world;
+  h->depth = sh.distance;
+}
 // The contact of a leaf whose test found one, into the job's manifold (in walk order).
 RSX_F void p3b_add_hit(ArenaState& S, const StaticData& D, P3bLoop& L, uint32_t tri, const LeafHit& h) {
   Ctx c = {S, D, L.unimplemented};

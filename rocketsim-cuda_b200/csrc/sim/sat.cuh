@@ -494,6 +494,123 @@ RSX_NOINL RSX_HD inline bool flat_tie(V3 h, const FeatPair* P, V3* r0, V3* r1) {
   return true;
 }
 
+// The SAT in three stages, for callers that spread the 47 feature pairs of one test over several threads:
+// sat_front runs the sweep and returns SAT_NO, SAT_HIT (out set) or SAT_PAIRS (the test goes on from f); the pairs are
+// feat_pair(f, 0..46) (enum_pairs' order); sat_back picks the closest pair, snaps flat ties and places the witness.
+// The three in a row compute what box_triangle_sat (below, one call, the serial callers' form) computes, bit for bit.
+struct SatFront {
+  Aff box_xf;
+  V3 hu, q[3], e[3], centroid, sep_axis;
+  float margin, maxd, best_gap;
+};
+enum { SAT_NO = 0, SAT_HIT = 1, SAT_PAIRS = 2 };
+RSX_F int sat_front(const Aff& box_xf, V3 hu, float margin, const V3 q[3], float maxd, SatHit* out, SatFront* f) {
+  V3 tmn = vmin(vmin(q[0], q[1]), q[2]), tmx = vmax(vmax(q[0], q[1]), q[2]);
+  for (int ax = 0; ax < 3; ++ax) {
+    float a = comp(tmn, ax), b = comp(tmx, ax), h = comp(hu, ax);
+    if (a > h) {
+      if (fsub(fsub(a, h), margin) >= maxd) return SAT_NO;
+    } else if (b < fneg(h) && fsub(fsub(fneg(h), b), margin) >= maxd) {
+      return SAT_NO;
+    }
+  }
+  V3 e0 = q[1] - q[0], e1 = q[2] - q[1], e2 = q[0] - q[2];
+  V3 fc = cross(e0, -e2);
+  float fl2 = len2(fc);
+  bool has_face = fl2 > 1e-20f;
+  V3 face = has_face ? fc / fsqrt(fl2) : vzero();
+  V3 centroid = (q[0] + q[1] + q[2]) * 0.33333334f;
+  V3 e[3] = {e0, e1, e2};
+  Sweep sw;
+  if (!sat_sweep(hu, q, tmn, tmx, e, face, has_face, centroid, margin, maxd, &sw)) return SAT_NO;
+  if (sw.has_sep) {
+    V3 nw = normalize_or_zero(box_xf.m * sw.sep_axis);
+    if (len2(nw) < 0.5f) return SAT_NO;
+    f->box_xf = box_xf;
+    f->hu = hu;
+    for (int i = 0; i < 3; ++i) {
+      f->q[i] = q[i];
+      f->e[i] = e[i];
+    }
+    f->centroid = centroid;
+    f->sep_axis = sw.sep_axis;
+    f->margin = margin;
+    f->maxd = maxd;
+    f->best_gap = sw.best_gap;
+    return SAT_PAIRS;
+  }
+  if (sw.best_overlap == kFltMax) return SAT_NO;
+  V3 n;
+  if (len2(sw.pen_axis) > 0.5f) {
+    n = sw.pen_axis;
+  } else if (has_face) {
+    float s = dot(face, -centroid);
+    n = s < 0.0f ? -face : face;
+  } else {
+    return SAT_NO;
+  }
+  float dist = fsub(fneg(sw.best_overlap), margin);
+  if (dist >= maxd) return SAT_NO;
+  V3 pb;
+  if (!pen_witness(hu, q, sw.kind, n, &pb))
+    if (!clipped_centroid(hu, q, &pb)) pb = tri_support(q, n);
+  V3 nw = normalize_or_zero(box_xf.m * n);
+  if (len2(nw) < 0.5f) return SAT_NO;
+  out->point_world = xform_point(box_xf, pb);
+  out->distance = dist;
+  return SAT_HIT;
+}
+// pair i of enum_pairs (0-2 clamped vertices, 3-10 corners in x / y / z bit order, 11-46 triangle edge x box edge)
+RSX_F FeatPair feat_pair(const SatFront& f, int i) {
+  const V3 h = f.hu;
+  if (i < 3) {
+    V3 pb = clamp_box(f.q[i], h);
+    return FeatPair{pb, f.q[i], len2(pb - f.q[i])};
+  }
+  if (i < 11) {
+    const int c = i - 3, ix = c >> 2, iy = (c >> 1) & 1, iz = c & 1;
+    V3 corner = v3(fmul(ix ? 1.0f : -1.0f, h.x), fmul(iy ? 1.0f : -1.0f, h.y), fmul(iz ? 1.0f : -1.0f, h.z));
+    V3 pt = closest_on_tri(corner, f.q, f.e[0], f.q[2] - f.q[0]);
+    return FeatPair{corner, pt, len2(corner - pt)};
+  }
+  const int c = i - 11, ti = c / 12, j = c % 12;
+  // box edge j of enum_pairs' table: corners (bit 0 x, bit 1 y, bit 2 z in its 0..7 numbering) of the edge's two ends
+  const int be[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  V3 cn[2];
+  for (int k = 0; k < 2; ++k) {
+    const int ci = be[j][k];  // enum_pairs' corner order: (-,-,-) (+,-,-) (+,+,-) (-,+,-), then the same at +z
+    const bool px = ci == 1 || ci == 2 || ci == 5 || ci == 6, py = ci == 2 || ci == 3 || ci == 6 || ci == 7, pz = ci >= 4;
+    cn[k] = v3(px ? h.x : fneg(h.x), py ? h.y : fneg(h.y), pz ? h.z : fneg(h.z));
+  }
+  V3 tp = f.q[ti], td = f.e[ti];
+  float ta = dot(td, td);
+  V3 ot, ob;
+  tri_edge_box_edge(tp, td, ta, cn[0], cn[1], &ot, &ob);
+  return FeatPair{ob, ot, len2(ob - ot)};
+}
+RSX_F bool sat_back(const SatFront& sf, const FeatPair* P, SatHit* out) {
+  FeatPair f = first_min(P);
+  if (len2(f.on_box - f.on_tri) > 1e-24f) {
+    float pl = len(f.on_box - f.on_tri);
+    V3 pb = f.on_tri;
+    bool snapped = false;
+    V3 s0, s1;
+    if (fsub(pl, sf.margin) < 0.0f && flat_tie(sf.hu, P, &s0, &s1)) {
+      pb = closest_on_seg(sf.centroid, s0, s1);
+      snapped = true;
+    }
+    float dist = snapped ? fsub(len(clamp_box(pb, sf.hu) - pb), sf.margin) : fsub(pl, sf.margin);
+    if (dist >= sf.maxd) return false;
+    out->point_world = xform_point(sf.box_xf, pb);
+    out->distance = dist;
+    return true;
+  }
+  V3 pb = tri_support(sf.q, sf.sep_axis);
+  out->point_world = xform_point(sf.box_xf, pb);
+  out->distance = fsub(sf.best_gap, sf.margin);
+  return true;
+}
+
 RSX_NOINL RSX_HD inline bool box_triangle_sat(const Aff& box_xf, V3 hu, float margin, const V3 q[3], float maxd, SatHit* out) {
   V3 tmn = vmin(vmin(q[0], q[1]), q[2]), tmx = vmax(vmax(q[0], q[1]), q[2]);
   for (int ax = 0; ax < 3; ++ax) {
@@ -516,9 +633,11 @@ RSX_NOINL RSX_HD inline bool box_triangle_sat(const Aff& box_xf, V3 hu, float ma
   if (sw.has_sep) {
     V3 nw = normalize_or_zero(box_xf.m * sw.sep_axis);
     if (len2(nw) < 0.5f) return false;
+    RSX_ZONE_BEGIN(z_fp);
     FeatPair P[kPairs];
     enum_pairs(hu, q, e, P);
     FeatPair f = first_min(P);
+    RSX_ZONE_END(z_fp, 4);
     if (len2(f.on_box - f.on_tri) > 1e-24f) {
       float pl = len(f.on_box - f.on_tri);
       V3 pb = f.on_tri;
