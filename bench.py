@@ -63,18 +63,13 @@ def _kc(rd, wr, inst, thr):
 
 
 KERNEL_COUNTERS = {
-    "k_sim8_multi": _kc(5205353728, 5090545920, 1597558738, 11031926045),
-    "k_sim8_lockstep_t448<7>": _kc(6368841216, 5860134400, 1615365164, 11353667488),
-    "k_sim8_lockstep_t512<7>": _kc(6355182592, 5853101056, 1615976108, 11372058856),
-    # splits 9 and 10: earlier captures by the same command with splits 7 / 9 / 10 and 7 / 10 / 11
-    "k_sim8_lockstep_t448<9>": _kc(6284846592, 5749324032, 1325706135, 11876194256),
-    "k_sim8_lockstep_t512<9>": _kc(6301496320, 5760274176, 1328764680, 11945208080),
-    "k_sim8_lockstep_t448<10>": _kc(6185998080, 5599560448, 1278761564, 11862062842),
-    "k_sim8_lockstep_t512<10>": _kc(6201578752, 5612222720, 1282169297, 11947769025),
-    "k_sim8_lockstep_t448<11>": _kc(6157746944, 5597323520, 1282829151, 11837348584),
-    "k_sim8_lockstep_t512<11>": _kc(6169138688, 5604822272, 1285928337, 11917567873),
-    "k_sim8_lockstep_t448<14>": _kc(5935916544, 5489462528, 1265547388, 12022290088),
-    "k_sim8_lockstep_t512<14>": _kc(5970577152, 5512242688, 1268913540, 12112352477),
+    "k_sim8_multi": _kc(5156746752, 5078530304, 1544248756, 10639862898),
+    "k_sim8_lockstep_t448<7>": _kc(6285861376, 5844596736, 1561873949, 10961083412),
+    "k_sim8_lockstep_t512<7>": _kc(6271582464, 5835747328, 1562452893, 10978506460),
+    "k_sim8_lockstep_t448<11>": _kc(6123927552, 5689207296, 1233322851, 11496541948),
+    "k_sim8_lockstep_t512<11>": _kc(6133884160, 5695117824, 1237386074, 11575349616),
+    "k_sim8_lockstep_t448<14>": _kc(5888915200, 5578572032, 1217817516, 11679509915),
+    "k_sim8_lockstep_t512<14>": _kc(5918841600, 5599824384, 1220777114, 11764147106),
 }
 
 
@@ -459,7 +454,7 @@ def tune_leg(leg, args, binning, seed, decisions, repeats):
     for s_ in range(args.warmup):
         run.step(leg.dctl[s_].data_ptr(), {"mode": "plain", "block": args.plain_block})
     tuned = run.tune([c.data_ptr() for c in tune_ctl], run.candidates(binning=binning), repeats=repeats)
-    top = [{"ms": round(ms, 3), "ms_repeats": [round(x, 3) for x in ts], **c} for ms, c, ts in tuned[:8]]
+    top = [{"ms_median": round(ms, 3), "ms_best": round(min(ts), 3), "ms_repeats": [round(x, 3) for x in ts], **c} for ms, c, ts in tuned[:8]]
     return dict(run.config), tuned, top
 
 
