@@ -63,13 +63,13 @@ def _kc(rd, wr, inst, thr):
 
 
 KERNEL_COUNTERS = {
-    "k_sim8_multi": _kc(5156746752, 5078530304, 1544248756, 10639862898),
-    "k_sim8_lockstep_t448<7>": _kc(6285861376, 5844596736, 1561873949, 10961083412),
-    "k_sim8_lockstep_t512<7>": _kc(6271582464, 5835747328, 1562452893, 10978506460),
-    "k_sim8_lockstep_t448<11>": _kc(6123927552, 5689207296, 1233322851, 11496541948),
-    "k_sim8_lockstep_t512<11>": _kc(6133884160, 5695117824, 1237386074, 11575349616),
-    "k_sim8_lockstep_t448<14>": _kc(5888915200, 5578572032, 1217817516, 11679509915),
-    "k_sim8_lockstep_t512<14>": _kc(5918841600, 5599824384, 1220777114, 11764147106),
+    "k_sim8_multi": _kc(5121808640, 5043499008, 1544248756, 10639862898),
+    "k_sim8_lockstep_t448<7>": _kc(6275417344, 5839662848, 1561873949, 10961083412),
+    "k_sim8_lockstep_t512<7>": _kc(6254316544, 5820695296, 1562420893, 10977538140),
+    "k_sim8_lockstep_t448<14>": _kc(5897723392, 5585730304, 1216579710, 11677240224),
+    "k_sim8_lockstep_t512<14>": _kc(5923618816, 5604210176, 1220573075, 11758854438),
+    "k_sim8_lockstep_t448<15>": _kc(5877837312, 5572951040, 1178267483, 11955292729),
+    "k_sim8_lockstep_t512<15>": _kc(5912239104, 5595661056, 1181828751, 12060642031),
 }
 
 
@@ -106,7 +106,7 @@ def parse():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--block", type=int, default=448, help="threads per block of the lockstep kernel")
     ap.add_argument("--grid", type=int, default=0, help="lockstep blocks (0: one per SM)")
-    ap.add_argument("--split", type=int, default=14,
+    ap.add_argument("--split", type=int, default=15,
                     help="lockstep barriers: 0 per phase, 1 + per car in P1, 2 + P1 in parts, 3 + per P3b step, 6 = 2 + P5 and P8 in parts, "
                          "7 = 6 + P3a per body, 9 = 7 + P3b's leaf tests pooled over the block, 10 = 9 + the wheel rays' mesh leaves pooled")
     ap.add_argument("--plain-block", type=int, default=32, help="threads per block of the plain launch (the reference's SIM8_BLOCK)")
@@ -548,7 +548,7 @@ def run_ours(args):
         Zs, Ys = [], []
         with torch.cuda.stream(run.stream):  # the copies on the stream the kernels wrote on
             for s in range(leg.steps):
-                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 14, "threshold": 0.5})
+                run.step(leg.dctl[s].data_ptr(), {"mode": "binned", "block": 448, "grid": run.sms, "split": 15, "threshold": 0.5})
                 Zs.append(run.Z.clone())
                 Ys.append(run.pred.labels(run.ev.data_ptr(), n).clone())
         run.stream.synchronize()
@@ -762,10 +762,10 @@ def large_leg(args, dev, pred, L):
 def profile_variants(args, leg):
     """For ncu captures at the headline size: 8 decisions of the plain launch from the start states (the states the bench
     times are later, contact-richer ones), then for the plain launch and each lockstep variant the autotuner considers
-    (blocks 448 / 512, splits 7 / 11 / 14), two decisions and then a third, each from those states.
+    (blocks 448 / 512, splits 7 / 14 / 15), two decisions and then a third, each from those states.
     Launch order: k_sim8_multi x 8, then 3 launches per variant in the order printed."""
     variants = [{"mode": "plain", "block": 32}] + [{"mode": "lockstep", "block": b, "grid": leg.run.sms, "split": s}
-                                                   for b in (448, 512) for s in (7, 11, 14)]
+                                                   for b in (448, 512) for s in (7, 14, 15)]
     run = leg.run
     run.restore(leg.start)
     for s in range(8):
@@ -809,7 +809,7 @@ def sweep(args, dev):
         t0 = time.perf_counter()
         run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
         train_s = time.perf_counter() - t0
-        base = {"block": 448, "grid": run.sms, "split": 14}
+        base = {"block": 448, "grid": run.sms, "split": 15}
         out, words = {}, {}
         for name, cfg in [("plain", {"mode": "plain", "block": 32}), ("lockstep", {"mode": "lockstep", **base}),
                           ("binned", {"mode": "binned", "threshold": 0.5, **base}),
@@ -933,7 +933,7 @@ def rollout_check(args, dev):
 
 
 ZONE_NAMES = {0: "P1 car pre-tick head", 1: "P1 wheel rays", 2: "P1 wheel response", 3: "P1 car pre-tick tail", 10: "P3b pair heads",
-              4: "  SAT: feature pairs (enumerate + first min)", 5: "  rays: candidates and mesh walks", 6: "  rays: pooled leaf evaluations",
+              4: "  SAT: feature pairs (enumerate + first min)", 5: "  rays: candidates and mesh walks", 9: "    rays: the mesh walks alone", 6: "  rays: pooled leaf evaluations",
               7: "  rays: replays and hits", 8: "  rays: pool barriers (incl. the prefix sum)", 11: "P3b box-triangle SAT", 12: "P3b box BVH step", 13: "P3b box job tail", 14: "P3b sphere BVH step",
               15: "P3b sphere-triangle", 16: "P3b sphere job tail", 17: "  head: convex-plane", 18: "  head: sphere-box",
               19: "  head: box-box", 21: "  head: sphere job begin", 22: "  head: box job begin", 23: "  head: near tail",

@@ -120,7 +120,8 @@ int rsx_sim8_persistent_ex(uint32_t* d_states, uint32_t n, const void* d_statics
  * split 9 with the wheel rays' mesh leaves pooled too (per car, every mesh candidate's leaves evaluated by all threads
  * in one round, the owners replaying them in candidate and walk order); split 11 is split 10 with P3a in one piece;
  * split 14 is split 11 with the 47 feature pairs of the box-triangle SATs that reach them computed by the whole block
- * (up to 18 SATs per round; the default: the fastest measured).  Register budget by block: up to 448 threads 144 registers, 512 128.  At
+ * (up to 18 SATs per round); split 15 is split 14 with the wheel rays' mesh walks run by the whole block level by level
+ * (their leaves sorted back into each walk's order; the default: the fastest measured).  Register budget by block: up to 448 threads 144 registers, 512 128.  At
  * most 2^24 arenas and grid 65,535 per call.  Results equal rsx_sim8_multi_raw's whatever grid, block, split or order. */
 #define RSX_LOCKSTEP_MAX_BLOCK 512u
 int rsx_sim8_lockstep_raw(uint32_t* d_states, uint32_t n, const void* d_statics, const uint8_t* d_sd_index,

@@ -286,8 +286,8 @@ int rsx_sim8_lockstep_ex(uint32_t* d_states, uint32_t n, const void* d_statics, 
                          uint32_t* d_result, uint32_t* d_event_or, const uint32_t* d_order, uint32_t* d_queue_counter, uint32_t grid,
                          uint32_t block, uint32_t split, uint32_t ticks_per_launch, void* stream) {
   if (!d_states || !d_statics || !d_controls || !d_result || !d_queue_counter || block < 32 || block > RSX_LOCKSTEP_MAX_BLOCK ||
-      (block & 31) || grid == 0 || (split > 11 && split != 14))
-    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep: null buffer, block not a multiple of 32 in 32..512, grid 0 or split not in 0..11, 14");
+      (block & 31) || grid == 0 || (split > 11 && split != 14 && split != 15))
+    return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep: null buffer, block not a multiple of 32 in 32..512, grid 0 or split not in 0..11, 14, 15");
   if (ticks_per_launch == 0 || RSX_TICKS_PER_DECISION % ticks_per_launch != 0)
     return rsx_set_last_error(RSX_E_ARG, "rsx_sim8_lockstep_ex: ticks_per_launch must divide 8 (1, 2, 4 or 8)");
   // idle warps claim 32 entries once per tick until their block ends: n plus that overshoot must stay below 2^32

@@ -12,7 +12,8 @@
 // the barriers out between P3b (4) or P4 (5) and P8, to measure what they buy), so that at any time the block's warps
 // fetch from one piece of code.  Splits 9 and 10 add the pooled contact work below; split 11 is split 10 with P3a in
 // one piece again (once P3b and the rays were pooled, P3a's per-body barriers cost more than they kept together);
-// split 14 is split 11 with the box-triangle SATs' feature pairs computed by the whole block.
+// split 14 is split 11 with the box-triangle SATs' feature pairs computed by the whole block; split 15 is split 14 with
+// the wheel rays' mesh walks run by the whole block level by level.
 //
 // Work: `gridDim.x` resident blocks (normally one per SM, `blockDim.x` up to RSX_LS_MAXT threads); every warp claims
 // 32 consecutive entries of `order` (arena indices; identity when null) with one atomicAdd on `counter` (zero at
@@ -92,11 +93,29 @@ struct RayPoolSmem {
   uint32_t pair_leaf[kRayPairs];
   sim::RayLeaf out[kRayPairs];
 };
-// one shared buffer for both pools (they serve different pieces of the tick) and the prefix sums
+// split 15: the wheel rays' mesh walks pooled too.  The block walks every mesh job's BVHs level by level (front: the
+// nodes of one level, each a slot | mesh << 6 | node << 10 and its path key); leaves go to a list (slot | mesh << 6 |
+// leaf << 10, key), a counting sort by slot and an insertion sort by key within each slot give every job its leaves in
+// the stack walk's order (sim/ray.cuh walk_expand).  Any list past its capacity sends the round to the serial walks.
+constexpr int kRayFront = 256;
+struct RayWalkSmem {
+  sim::RayMeshJob job[kRayJobs];
+  const StaticData* jd[kRayJobs];
+  Box3 jbox[kRayJobs];
+  uint32_t jbody[kRayJobs];
+  uint32_t cnt[kRayJobs], seg[kRayJobs], fill[kRayJobs];
+  uint32_t leaf_a[kRayPairs], key_a[kRayPairs];  // as found
+  uint32_t leaf_b[kRayPairs], key_b[kRayPairs];  // by slot, then by key
+  sim::RayLeaf out[kRayPairs];
+  uint32_t front[2][kRayFront][2];
+  uint32_t nfront[sim::kWalkLevels + 1], nleaf, ovf;
+};
+// one shared buffer for the pools (they serve different pieces of the tick) and the prefix sums
 struct Pools {
   union {
     PoolSmem p3b;
     RayPoolSmem rays;
+    RayWalkSmem walk;
   };
   uint32_t warp_sum[32];
   uint32_t limit;
@@ -265,6 +284,7 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
   uint8_t meshes[kRayLeavesLane], jcand[kRayJobsLane], jstart[kRayJobsLane], jcount[kRayJobsLane];
   int nj = 0, nl = 0;
   bool fits = true;
+  RSX_ZONE_BEGIN(zr6);
   for (int k = 0; k < nk && fits; ++k) {
     const uint32_t w = cand[k];
     const uint32_t shape = D->bodies[w].shape;
@@ -295,6 +315,7 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
     jcount[nj] = (uint8_t)(nl - first);
     ++nj;
   }
+  RSX_ZONE_END(zr6, 9);
   if (!fits) nj = nl = 0;
   RSX_ZONE_END(zr0, 5);
   RSX_ZONE_BEGIN(zr1);
@@ -352,9 +373,186 @@ __device__ __noinline__ void rays_pooled(ArenaState& s, const StaticData* D, boo
   }
   RSX_ZONE_END(zr4, 7);
   RSX_ZONE_BEGIN(zr5);
-  __syncthreads();
-  RSX_ZONE_END(zr5, 8);  // the pool is read above: the next piece's writes come after every lane's reads
+  __syncthreads();  // the pool is read above: the next piece's writes come after every lane's reads
+  RSX_ZONE_END(zr5, 8);
 }
+
+// rays_pooled with the mesh walks pooled too (split 15); every thread of the block calls it.  Each lane's mesh
+// candidates (up to kRayJobsLane) become jobs in shared memory, the block walks all their BVHs level by level, sorts
+// each job's leaves into the stack walk's order, evaluates them, and each owner replays its candidates in order as in
+// rays_pooled.  Results equal vehicle_rays'.
+__device__ __noinline__ void rays_pooled_walk(ArenaState& s, const StaticData* D, bool act, int ci, sim::WheelHit hits[kWheels]) {
+  Pools& u = pools();
+  RayWalkSmem& sm = u.walk;
+  sim::RayPacket pk;
+  uint32_t cand[kHandles];
+  int nk = 0;
+  RSX_ZONE_BEGIN(zr0);
+  if (act) {
+    sim::vehicle_rays_begin(s, *D, ci, pk);
+    nk = sim::grid_candidates(s, *D, &pk, cand);
+  }
+  uint8_t jcand[kRayJobsLane];
+  int nj = 0;
+  for (int k = 0; k < nk; ++k) {
+    const uint32_t shape = D->bodies[cand[k]].shape;
+    if (shape == sim::SHAPE_BOX || shape == sim::SHAPE_SPHERE || shape == sim::SHAPE_PLANE) continue;
+    if (nj == kRayJobsLane) {  // more mesh bodies than a lane may pool: this lane walks its own
+      nj = -1;
+      break;
+    }
+    jcand[nj++] = (uint8_t)k;
+  }
+  const bool mine = nj > 0;
+  if (nj < 0) nj = 0;
+  RSX_ZONE_END(zr0, 5);
+  RSX_ZONE_BEGIN(zr1);
+  uint32_t total;
+  const uint32_t slot = block_scan((uint32_t)nj, &total, u);
+  // pooled lanes are a prefix in scan order, so the jobs are slots [0, limit)
+  const bool pooled = mine && slot + (uint32_t)nj <= (uint32_t)kRayJobs;
+  if (threadIdx.x == 0) {
+    for (int l = 0; l <= sim::kWalkLevels; ++l) sm.nfront[l] = 0;
+    sm.nleaf = 0;
+    sm.ovf = 0;
+  }
+  if (pooled) {
+    for (int j = 0; j < nj; ++j) {  // no body has been tested yet: the packet's fractions are all still 1
+      const uint32_t w = cand[jcand[j]], q = slot + (uint32_t)j;
+      sim::LocalRays lr;
+      sim::RayBox rb;
+      sim::ray_body_setup(s, *D, w, &pk, lr, rb);
+      sim::ray_mesh_job(lr, rb, sm.job[q]);
+      sm.jd[q] = D;
+      sm.jbox[q] = rb.box;
+      sm.jbody[q] = w;
+      sm.cnt[q] = 0;
+      sm.fill[q] = 0;
+    }
+    atomicMax(&u.limit, slot + (uint32_t)nj);
+  }
+  __syncthreads();
+  RSX_ZONE_END(zr1, 8);
+  RSX_ZONE_BEGIN(zr6);
+  const uint32_t J = u.limit;
+  // the jobs' meshes: every mesh of the job's body whose root box meets the job's box, in mesh order by key
+  for (uint32_t i = threadIdx.x; i < J * (uint32_t)kMeshes; i += blockDim.x) {
+    const uint32_t q = i / (uint32_t)kMeshes;
+    const int m = (int)(i % (uint32_t)kMeshes);
+    const StaticData& Dj = *sm.jd[q];
+    if (Dj.meshes[m].body == sm.jbody[q] && box_overlap(sm.jbox[q], Dj.meshes[m].root_box)) {
+      const uint32_t f = atomicAdd(&sm.nfront[0], 1u);
+      if (f < (uint32_t)kRayFront) {
+        sm.front[0][f][0] = q | ((uint32_t)m << 6);
+        sm.front[0][f][1] = sim::walk_root_key(m);
+      } else {
+        sm.ovf = 1;
+      }
+    }
+  }
+  __syncthreads();
+  for (int level = 0; level < sim::kWalkLevels; ++level) {
+    const uint32_t F = sm.nfront[level];
+    if (F == 0 || sm.ovf) break;  // (uniform: read after the barrier, written only between barriers)
+    const int cur = level & 1;
+    for (uint32_t i = threadIdx.x; i < F; i += blockDim.x) {
+      const uint32_t it = sm.front[cur][i][0], key = sm.front[cur][i][1];
+      const uint32_t q = it & 63u, m = (it >> 6) & 15u, node = it >> 10;
+      sim::walk_expand(*sm.jd[q], (int)m, node, key, level, sm.jbox[q], [&](uint32_t ch, uint32_t k2) {
+        if (ch & 0x80000000u) {
+          const uint32_t e = atomicAdd(&sm.nleaf, 1u);
+          if (e < (uint32_t)kRayPairs) {
+            sm.leaf_a[e] = q | (m << 6) | ((ch & 0x7FFFFFFFu) << 10);
+            sm.key_a[e] = k2;
+            atomicAdd(&sm.cnt[q], 1u);
+          } else {
+            sm.ovf = 1;
+          }
+        } else {
+          const uint32_t f = atomicAdd(&sm.nfront[level + 1], 1u);
+          if (f < (uint32_t)kRayFront) {
+            sm.front[cur ^ 1][f][0] = q | (m << 6) | (ch << 10);
+            sm.front[cur ^ 1][f][1] = k2;
+          } else {
+            sm.ovf = 1;
+          }
+        }
+      });
+    }
+    __syncthreads();
+  }
+  // past a list's capacity, or a tree deeper than the keys hold: every lane walks its own this round
+  const bool walked = !(sm.ovf || sm.nfront[sim::kWalkLevels] != 0);
+  const uint32_t nl = walked ? sm.nleaf : 0u;
+  if (walked) {
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0;
+      for (uint32_t q = 0; q < J; ++q) {
+        sm.seg[q] = acc;
+        acc += sm.cnt[q];
+      }
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < nl; e += blockDim.x) {
+      const uint32_t q = sm.leaf_a[e] & 63u;
+      const uint32_t at = sm.seg[q] + atomicAdd(&sm.fill[q], 1u);
+      sm.leaf_b[at] = sm.leaf_a[e];
+      sm.key_b[at] = sm.key_a[e];
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < J; q += blockDim.x) {  // each job's leaves into key order
+      const uint32_t b = sm.seg[q], n = sm.cnt[q];
+      for (uint32_t i = 1; i < n; ++i) {
+        const uint32_t lv = sm.leaf_b[b + i], kv = sm.key_b[b + i];
+        uint32_t j = i;
+        for (; j > 0 && sm.key_b[b + j - 1] > kv; --j) {
+          sm.leaf_b[b + j] = sm.leaf_b[b + j - 1];
+          sm.key_b[b + j] = sm.key_b[b + j - 1];
+        }
+        sm.leaf_b[b + j] = lv;
+        sm.key_b[b + j] = kv;
+      }
+    }
+    __syncthreads();
+  }
+  RSX_ZONE_END(zr6, 9);
+  RSX_ZONE_BEGIN(zr2);
+  for (uint32_t e = threadIdx.x; e < nl; e += blockDim.x) {
+    const uint32_t v = sm.leaf_b[e], q = v & 63u;
+    const StaticData& Dj = *sm.jd[q];
+    sim::ray_leaf_eval(sm.job[q], Dj, Dj.meshes[(v >> 6) & 15u], v >> 10, nullptr, &sm.out[e]);
+  }
+  RSX_ZONE_END(zr2, 6);
+  RSX_ZONE_BEGIN(zr3);
+  __syncthreads();
+  RSX_ZONE_END(zr3, 8);
+  RSX_ZONE_BEGIN(zr4);
+  if (act) {
+    int j = 0;
+    for (int k = 0; k < nk; ++k) {
+      const uint32_t w = cand[k];
+      if (walked && pooled && j < nj && jcand[j] == k) {
+        sim::LocalRays lr;
+        sim::RayBox rb;
+        sim::ray_body_setup(s, *D, w, &pk, lr, rb);
+        const uint32_t q = slot + (uint32_t)j, b = sm.seg[q], n = sm.cnt[q];
+        for (uint32_t t = 0; t < n; ++t) {
+          const uint32_t v = sm.leaf_b[b + t];
+          sim::ray_leaf_replay(&lr, rb.lmax, *D, D->meshes[(v >> 6) & 15u], v >> 10, sm.out[b + t]);
+        }
+        ++j;
+      } else {
+        sim::ray_body(s, *D, w, &pk);
+      }
+    }
+    sim::wheel_packet_hits(s, *D, pk, hits);
+  }
+  RSX_ZONE_END(zr4, 7);
+  RSX_ZONE_BEGIN(zr5);
+  __syncthreads();  // the pool is read above: the next piece's writes come after every lane's reads
+  RSX_ZONE_END(zr5, 8);
+}
+
 }  // namespace
 
 template <int SPLIT>
@@ -446,7 +644,9 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
         sim::WheelHit hits[kWheels];
         {
           RSX_ZONE_BEGIN(z2);
-          if (SPLIT >= 10)
+          if (SPLIT >= 15)
+            rays_pooled_walk(s, D, have && act, ci, hits);
+          else if (SPLIT >= 10)
             rays_pooled(s, D, have && act, ci, hits);
           else if (have && act)
             sim::vehicle_rays(s, *D, ci, hits);
@@ -520,7 +720,7 @@ __global__ void __launch_bounds__(RSX_LS_MAXT, 1) K_NAME(uint32_t* states, const
           continue;
         }
         if (SPLIT >= 9 && k == 4) {  // P3b with the block's leaf tests pooled
-          p3b_pooled<SPLIT == 14>(s, D, have, &un);
+          p3b_pooled<(SPLIT >= 14)>(s, D, have, &un);
           continue;
         }
         if (SPLIT == 3 && k == 4) {
@@ -604,6 +804,7 @@ cudaError_t L_NAME(uint32_t* states, const void* sds, const uint8_t* sd_index, c
   const Controls* C = (const Controls*)controls;
 #define RSX_LS_LAUNCH(k) K_NAME<k><<<grid, block, 0, s>>>(states, D, sd_index, C, result, ev_or, order, counter, n, t_first, t_last)
   switch (split) {
+    case 15: RSX_LS_LAUNCH(15); break;
     case 14: RSX_LS_LAUNCH(14); break;
     case 11: RSX_LS_LAUNCH(11); break;
     case 10: RSX_LS_LAUNCH(10); break;

@@ -223,6 +223,21 @@ RSX_F bool ray_walk_next(RayWalk& w, const StaticData& D, uint32_t body, const B
   }
   return false;
 }
+// ---- a mesh body's walk level by level, for callers that expand many walks' nodes side by side ----
+// An item of the walk is a node of one of the body's meshes with its path key: the mesh index in bits 12-15 and, for
+// each level below the mesh's root, the index (0-3) of the child taken, two bits from bit 10 down.  The stack walk of
+// ray_walk_next takes the meshes in index order and, within a mesh, a child's whole subtree before the next child's,
+// so sorting a walk's leaves by key gives ray_walk_next's order.  Keys hold kWalkLevels levels of children.
+constexpr int kWalkLevels = 6;
+RSX_F uint32_t walk_root_key(int mesh) { return (uint32_t)mesh << 12; }
+// the children of node `node` of mesh m (level 0: the root) whose boxes meet box, in child order: emit(child, key)
+template <class Emit>
+RSX_F void walk_expand(const StaticData& D, int m, uint32_t node, uint32_t key, int level, const Box3& box, Emit&& emit) {
+  const WideNode& nd = D.nodes[D.meshes[m].node_first + node];
+  const uint32_t mk = node_mask(nd, box);
+  for (int l = 0; l < (int)nd.n_child; ++l)
+    if (mk & (1u << l)) emit(nd.child[l], key | ((uint32_t)l << (10 - 2 * level)));
+}
 // the whole test of a mesh body, leaf by leaf
 RSX_HD RSX_NOINL inline void ray_mesh_body(const StaticData& D, uint32_t body, LocalRays* lr, RayBox* rb) {
   RayMeshJob j;

@@ -130,7 +130,7 @@ def main():
     t0 = time.perf_counter()
     run.train_predictor(control_seed=args.seed * 1000 + 500, decisions=max(2, 2097152 // n))
     train_s = time.perf_counter() - t0
-    cfg = {"mode": args.order, "block": 448, "grid": run.sms, "split": 14, "threshold": 0.5}
+    cfg = {"mode": args.order, "block": 448, "grid": run.sms, "split": 15, "threshold": 0.5}
     if args.order == "levels":
         cfg.update({"levels": 16, "weights": [1.0] * 6})
     ro = Rollout(run, pool, reset_seed=args.seed * 7919, mix=mix, config=cfg)

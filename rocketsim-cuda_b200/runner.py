@@ -52,7 +52,7 @@ class DecisionRunner:
         self.Z = t.zeros((n, 8), dtype=t.float32, device=dev.device)
         self.sms = torch.cuda.get_device_properties(dev.device).multi_processor_count
         self.pred = None
-        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 14, "threshold": None}
+        self.config = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 15, "threshold": None}
         torch.cuda.synchronize(dev.device)
 
     # ---- observations and rewards of the last decision ----
@@ -146,7 +146,7 @@ class DecisionRunner:
             self.pred = P.ContactPredictor(self.dev.device, seed=seed, stream=self.sptr)
         snap = self.snapshot()
         Xs, Ys = [], []
-        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 14}
+        cfg = {"mode": "lockstep", "block": 448, "grid": self.sms, "split": 15}
         for d in range(decisions):
             ctl = t.from_numpy(rsx.decision_controls(control_seed, d, self.n).view(np.int32)).to(self.dev.device, non_blocking=False)
             self.stream.wait_stream(t.cuda.current_stream(self.dev.device))
@@ -176,14 +176,14 @@ class DecisionRunner:
         # the persistent kernel without barriers: register budget (min_blocks of 64 threads per SM) and queue granularity
         for min_blocks, gran in ((8, 1), (8, 4), (12, 1)):
             out.append({"mode": "persistent", "block": 64, "grid": self.sms * min_blocks, "granularity": gran, "min_blocks": min_blocks})
-        # splits: 7 (lockstep), 11 (+ P3b's mesh-leaf tests and the wheel rays' mesh leaves pooled over the block, P3a in
-        # one piece), 14 (11 with the SATs' feature pairs spread over the block)
-        for block, split in itertools.product((448, 512), (7, 11, 14)):
+        # splits: 7 (lockstep), 14 (+ P3b's mesh-leaf tests, the SATs' feature pairs and the wheel rays' mesh leaves
+        # pooled over the block, P3a in one piece), 15 (14 with the wheel rays' mesh walks pooled too)
+        for block, split in itertools.product((448, 512), (7, 14, 15)):
             out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None})
-            if split == 14:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
+            if split == 15:  # ticks per launch: a decision in 2 or 4 launches, arenas re-claimed (re-balanced) between them
                 for ticks in (4, 2):
                     out.append({"mode": "lockstep", "block": block, "grid": self.sms, "split": split, "threshold": None, "ticks": ticks})
-            if binning and self.pred is not None and split >= 11:
+            if binning and self.pred is not None and split >= 14:
                 for thr, labels in ((0.3, P.ALL_LABELS), (0.5, P.ALL_LABELS)):
                     out.append({"mode": "binned", "block": block, "grid": self.sms, "split": split, "threshold": thr, "labels": labels})
                 out.append({"mode": "levels", "block": block, "grid": self.sms, "split": split, "threshold": None, "levels": 16,

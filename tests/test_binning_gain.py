@@ -3,7 +3,7 @@ order and over the trained network's orders (two bins, sixteen cost levels), 262
 (several claim rounds per SM, where the order matters), timed on the same decisions from the same start states.  The
 test checks what must hold — every order gives the same words, and the trained network's recall and precision on
 these decisions — and prints the timings (run with -s to see them); the speed-ups are measurements, not pass
-conditions.  With the lockstep kernel's pooled contact work (splits 9 to 14) the heavy arenas' leaf tests are spread over
+conditions.  With the lockstep kernel's pooled contact work (splits 9 to 15) the heavy arenas' leaf tests are spread over
 the block, and the orders measure within a few percent of the identity order either way (best of three, 262,144 and
 1,048,576 arenas after 8 decisions: two bins +0.7% / +2.2%, sixteen levels -1.5% / +0.8%), inside the spread of
 repeated runs, so no gain is asserted."""
@@ -47,7 +47,7 @@ def test_trained_order_gain_is_measured_and_exact(rsx):
             e1.synchronize()
             return e0.elapsed_time(e1), run.snapshot().cpu().numpy(), run.res.cpu().numpy().copy()
 
-        base = {"block": 448, "grid": run.sms, "split": 14}
+        base = {"block": 448, "grid": run.sms, "split": 15}
         for_warm = timed({"mode": "lockstep", **base})  # first launches load the kernels
         t_id, w_id, r_id = timed({"mode": "lockstep", **base})
         t_un, w_un, r_un = timed({"mode": "binned", "threshold": 0.5, **base})

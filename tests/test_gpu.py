@@ -115,7 +115,8 @@ def test_result_independent_of_block_order_and_queue(rsx, dev):
                 ("lock", 448, dperm, 148, 6), ("lock", 96, None, 2, 6), ("lock", 448, None, 148, 4), ("lock", 64, dperm, 2, 5),
                 ("lock", 448, dperm, 148, 7), ("lock", 448, dperm, 148, 9), ("lock", 96, None, 2, 9), ("lock", 512, None, 5, 9),
                 ("lock", 448, dperm, 148, 10), ("lock", 64, None, 3, 10), ("lock", 448, dperm, 148, 11), ("lock", 96, None, 2, 11),
-                ("lock", 512, None, 5, 11), ("lock", 448, dperm, 148, 14), ("lock", 64, None, 3, 14), ("lock", 512, None, 5, 14)]
+                ("lock", 512, None, 5, 11), ("lock", 448, dperm, 148, 14), ("lock", 64, None, 3, 14), ("lock", 512, None, 5, 14),
+                ("lock", 448, dperm, 148, 15), ("lock", 96, None, 2, 15), ("lock", 512, None, 5, 15)]
     for kind, block, order, grid, gran in variants:
         ds = dev.upload_states(st)
         res = dev.alloc_result(n)
@@ -177,7 +178,7 @@ def test_ticks_per_launch_same_words(rsx, dev):
         for d in range(6):
             ctl = dev.upload_controls(rsx.decision_controls(13, d, n))
             rsx.check(L.rsx_sim8_lockstep_ex(ds.ptr(), n, dsd.ptr(), didx.data_ptr(), ctl.data_ptr(), res.data_ptr(), ev.data_ptr(),
-                                             order.data_ptr() if order is not None else None, counter.data_ptr(), grid, block, 14, ticks,
+                                             order.data_ptr() if order is not None else None, counter.data_ptr(), grid, block, 15, ticks,
                                              dev.stream_ptr()), f"lockstep ticks {ticks}")
             dev.sync()
             scored += int(((res.cpu().numpy().view(np.uint32) & 0xFF) != 0).sum())

@@ -39,7 +39,7 @@ def test_rollout_with_retraining_and_resets_matches_oracle(rsx):
             if d + 1 in checks:
                 got[d + 1] = dev.download_states(run.ds)[sample]
 
-        cfg = {"mode": "binned", "block": 448, "grid": run.sms, "split": 14, "threshold": 0.5}
+        cfg = {"mode": "binned", "block": 448, "grid": run.sms, "split": 15, "threshold": 0.5}
         ro = rollout.Rollout(run, pool, reset_seed=99, mix=mix, config=cfg, sample_per_decision=8192)
         windows = ro.run_decisions(D, retrain_every=16, on_decision=on_decision)
         assert len(windows) == 3 and windows[-1]["decisions"] == [32, 39]
@@ -94,7 +94,7 @@ def test_long_levels_rollout_matches_oracle_on_a_sample(rsx):
             if d + 1 in checks:
                 got[d + 1] = dev.download_states(run.ds)[sample]
 
-        cfg = {"mode": "levels", "block": 448, "grid": run.sms, "split": 14, "threshold": None, "levels": 16, "weights": [1.0] * 6}
+        cfg = {"mode": "levels", "block": 448, "grid": run.sms, "split": 15, "threshold": None, "levels": 16, "weights": [1.0] * 6}
         ro = rollout.Rollout(run, pool, reset_seed=123, mix=mix, config=cfg, sample_per_decision=8192)
         windows = ro.run_decisions(D, retrain_every=20, on_decision=on_decision)
         assert len(windows) == 3 and all(w["overflow"] == 0 and w["unimplemented"] == 0 for w in windows)
