@@ -288,6 +288,20 @@ RSX_F void cell_indices(const StaticData& D, V3 p, uint32_t out[3]) {
   }
 }
 RSX_F uint32_t cell_of(const StaticData& D, const uint32_t i[3]) { return i[0] * D.grid_n[1] * D.grid_n[2] + i[1] * D.grid_n[2] + i[2]; }
+// The first entry of the ray grid's dynamic list at or after cell c.  The list is sorted by cell (broad.cuh dyn_cells_block inserts
+// after every entry of a lower or equal cell and removes in place), so a cell's entries are one run from here, in list
+// order: the entries a scan of the whole list for the cell meets, in the same order.
+RSX_F uint32_t dyn_cells_first(const ArenaState& S, uint32_t c) {
+  uint32_t lo = 0, hi = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (S.dyn_cells[mid].cell < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
 
 }  // namespace sim
 }  // namespace rsx

@@ -173,14 +173,22 @@ RSX_F void dyn_block_range(const StaticData& D, const uint32_t idx[3], uint32_t 
     hi[a] = top < p ? top : p;
   }
 }
-RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_t h, const uint32_t idx[3]) {
+// keep_freed (a removal followed at once by the insertion of the same handle): the freed slots are not zeroed here;
+// the caller zeroes those the insertion does not refill (dyn_cells_zero_from), which leaves the same words.
+RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_t h, const uint32_t idx[3], bool keep_freed = false) {
   uint32_t lo[3], hi[3];
   dyn_block_range(D, idx, lo, hi);
   const uint32_t ny = D.grid_n[1], nz = D.grid_n[2];
   if (!add) {
     uint32_t removed = 0;  // bit (i - lo0) * 9 + (j - lo1) * 3 + (k - lo2): that cell's entry is gone
-    uint32_t n = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells, w = 0;
-    for (uint32_t r = 0; r < n; ++r) {
+    uint32_t n = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells;
+    // the list is sorted by cell, and every cell of the block is at least the block's first: the entries before the
+    // first at or after that cell stay where they are
+    const uint32_t lo3[3] = {lo[0], lo[1], lo[2]};
+    uint32_t r0 = dyn_cells_first(S, cell_of(D, lo3));
+    if (r0 > n) r0 = n;
+    uint32_t w = r0;
+    for (uint32_t r = r0; r < n; ++r) {
       DynCell e = S.dyn_cells[r];
       if (e.handle == h) {
         uint32_t i = e.cell / (ny * nz), j = (e.cell / nz) % ny, k = e.cell % nz;
@@ -195,7 +203,8 @@ RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_
       if (w != r) S.dyn_cells[w] = e;
       ++w;
     }
-    for (uint32_t r = w; r < n; ++r) S.dyn_cells[r] = DynCell{0, 0};
+    if (!keep_freed)
+      for (uint32_t r = w; r < n; ++r) S.dyn_cells[r] = DynCell{0, 0};
     S.n_dyn_cells = w;
     return;
   }
@@ -222,6 +231,11 @@ RSX_F void dyn_cells_block(ArenaState& S, const StaticData& D, bool add, uint32_
     }
   }
   S.n_dyn_cells = n + take;
+}
+
+// zero the list's slots [S.n_dyn_cells, end) (end: the count before a keep_freed removal)
+RSX_F void dyn_cells_zero_from(ArenaState& S, uint32_t end) {
+  for (uint32_t r = S.n_dyn_cells; r < end; ++r) S.dyn_cells[r] = DynCell{0, 0};
 }
 
 RSX_F Box3 dyn_shape_box(const BodyConst& c, const Aff& t) {
@@ -254,11 +268,13 @@ RSX_F void phase3a_body(ArenaState& S, const StaticData& D, uint32_t d) {
     uint32_t nc = cell_of(D, ni);
     S.dyn_proxy[d].cell = nc;
     if (nc != old) {
-      dyn_cells_block(S, D, false, h, S.dyn_proxy[d].idx);
+      const uint32_t before = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells;
+      dyn_cells_block(S, D, false, h, S.dyn_proxy[d].idx, true);
       S.dyn_proxy[d].idx[0] = ni[0];
       S.dyn_proxy[d].idx[1] = ni[1];
       S.dyn_proxy[d].idx[2] = ni[2];
       dyn_cells_block(S, D, true, h, ni);
+      dyn_cells_zero_from(S, before);
     }
   }
 }

@@ -548,20 +548,6 @@ RSX_F bool ray_accepts(const StaticData& D, uint32_t h, const RayPacket* pk) {
   return (px.group & pk->mask) != 0 && (pk->group & px.mask) != 0;
 }
 
-// The first entry of the ray grid's dynamic list at or after cell c.  The list is sorted by cell (dyn_cells_block inserts
-// after every entry of a lower or equal cell and removes in place), so a cell's entries are one run from here, in list
-// order: the entries a scan of the whole list for the cell meets, in the same order.
-RSX_F uint32_t dyn_cells_first(const ArenaState& S, uint32_t c) {
-  uint32_t lo = 0, hi = S.n_dyn_cells;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (S.dyn_cells[mid].cell < c)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
-}
 // the grid's candidate walk: one cell per distinct ray source, its static handles, then its dynamic ones
 // the candidate bodies of the packet, in the walk's order (nothing in the walk depends on the hits); returns their count
 RSX_F int grid_candidates(const ArenaState& S, const StaticData& D, const RayPacket* pk, uint32_t cand[kHandles]) {
@@ -584,6 +570,7 @@ RSX_F int grid_candidates(const ArenaState& S, const StaticData& D, const RayPac
   }
   uint32_t seen = 0;
   int nk = 0;
+  const uint32_t nd = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells;
   for (int ci = 0; ci < nc; ++ci) {
     uint32_t cell = cells[ci];
     const CellRange& cr = D.cells[cell];
@@ -593,7 +580,7 @@ RSX_F int grid_candidates(const ArenaState& S, const StaticData& D, const RayPac
       seen |= 1u << h;
       if (box_overlap(rbx, proxy_box(S, D, h)) && ray_accepts(D, h, pk)) cand[nk++] = D.proxies[h].body;
     }
-    for (uint32_t e = dyn_cells_first(S, cell); e < S.n_dyn_cells && S.dyn_cells[e].cell == cell; ++e) {
+    for (uint32_t e = dyn_cells_first(S, cell); e < nd && S.dyn_cells[e].cell == cell; ++e) {
       uint32_t h = S.dyn_cells[e].handle;
       if (seen & (1u << h)) continue;
       seen |= 1u << h;

@@ -125,3 +125,108 @@ def test_dynamic_cell_search_equals_scan(tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
     words = out.stdout.split()
     assert int(words[words.index("dynamic-candidates") + 1]) > 100, out.stdout  # the dynamic entries were exercised
+
+
+P3A_PROGRAM = r"""
+#include <cstdio>
+#include <cstring>
+#include <cstdint>
+#include <vector>
+#include "state.cuh"
+#include "sim/physics.cuh"
+using namespace rsx;
+extern "C" int rsx_build_static(uint32_t* words, uint64_t seed, int p0, int p1);
+extern "C" int rsx_make_states_multi(const uint32_t* sds, uint32_t count, const uint8_t* idx, uint32_t* out, uint32_t n,
+                                     uint64_t seed, const float* mix);
+// a body's move to another cell as the list rule states it: the old block's entries out (a pass over the whole list,
+// freed slots zeroed), then the new block's in
+static void move_plain(ArenaState& S, const StaticData& D, uint32_t h, const uint32_t old_idx[3], const uint32_t new_idx[3]) {
+  uint32_t lo[3], hi[3];
+  sim::dyn_block_range(D, old_idx, lo, hi);
+  const uint32_t ny = D.grid_n[1], nz = D.grid_n[2];
+  uint32_t removed = 0, n = S.n_dyn_cells < (uint32_t)kMaxDynCells ? S.n_dyn_cells : (uint32_t)kMaxDynCells, w = 0;
+  for (uint32_t r = 0; r < n; ++r) {
+    DynCell e = S.dyn_cells[r];
+    if (e.handle == h) {
+      uint32_t i = e.cell / (ny * nz), j = (e.cell / nz) % ny, k = e.cell % nz;
+      if (i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2]) {
+        uint32_t bit = 1u << ((i - lo[0]) * 9 + (j - lo[1]) * 3 + (k - lo[2]));
+        if (!(removed & bit)) { removed |= bit; continue; }
+      }
+    }
+    if (w != r) S.dyn_cells[w] = e;
+    ++w;
+  }
+  for (uint32_t r = w; r < n; ++r) S.dyn_cells[r] = DynCell{0, 0};
+  S.n_dyn_cells = w;
+  sim::dyn_cells_block(S, D, true, h, new_idx);
+}
+int main() {
+  const int n = 3072, decisions = 10;
+  std::vector<uint32_t> sds((size_t)49 * kStaticWords);
+  for (int p = 0; p < 7; ++p)
+    for (int q = 0; q < 7; ++q) rsx_build_static(&sds[(size_t)(p * 7 + q) * kStaticWords], 7, p, q);
+  std::vector<uint8_t> idx(n);
+  for (int a = 0; a < n; ++a) idx[a] = (uint8_t)((a * 37u + 11u) % 49u);
+  std::vector<uint32_t> st((size_t)n * kArenaWords);
+  const float mix[5] = {0.1f, 0.3f, 0.2f, 0.3f, 0.1f};
+  rsx_make_states_multi(sds.data(), 49, idx.data(), st.data(), n, 5, mix);
+  long moves = 0, differ = 0;
+  ArenaState* T = new ArenaState;
+  for (int a = 0; a < n; ++a) {
+    ArenaState& S = *reinterpret_cast<ArenaState*>(&st[(size_t)a * kArenaWords]);
+    const StaticData& D = *reinterpret_cast<const StaticData*>(&sds[(size_t)idx[a] * kStaticWords]);
+    for (int t = 0; t < decisions * 8; ++t) {
+      for (int c = 0; c < 2; ++c) {
+        Controls& k = S.cars[c].controls;
+        k.throttle = 1.0f;
+        k.steer = (float)(((a * 7 + t / 9 + c) % 3) - 1);
+        k.boost = ((a + t / 2 + c) % 2) == 0;
+        k.jump = ((a + t / 7 + c) % 6) == 0;
+      }
+      sim::t_p0(S, D); sim::t_p1(S, D); sim::t_p2(S, D);
+      // every body's move this tick, replayed on a copy by the plain rule from the same list
+      std::memcpy(T, &S, sizeof S);
+      sim::t_p3a(S, D);
+      for (uint32_t d = 0; d < (uint32_t)kDyn; ++d) {
+        if (S.dyn_proxy[d].cell == T->dyn_proxy[d].cell) continue;
+        ++moves;
+        move_plain(*T, D, D.dyn_handle[d], T->dyn_proxy[d].idx, S.dyn_proxy[d].idx);
+        for (int x = 0; x < 3; ++x) T->dyn_proxy[d].idx[x] = S.dyn_proxy[d].idx[x];
+        T->dyn_proxy[d].cell = S.dyn_proxy[d].cell;
+      }
+      if (std::memcmp(T->dyn_cells, S.dyn_cells, sizeof S.dyn_cells) != 0 || T->n_dyn_cells != S.n_dyn_cells ||
+          T->overflow[OVF_DYN_CELLS] != S.overflow[OVF_DYN_CELLS]) ++differ;
+      sim::t_p3b(S, D); sim::t_p4(S, D); sim::t_p5(S, D); sim::t_p6(S, D); sim::t_p7(S, D); sim::t_p8(S, D);
+    }
+  }
+  std::printf("moves %ld differ %ld\n", moves, differ);
+  return differ != 0;
+}
+"""
+
+
+def test_cell_moves_equal_plain_list_rule(tmp_path):
+    """P3a's update of the dynamic-cell list when a body changes cell (the removal started at the old block's first
+    cell, the freed slots zeroed once after the insertion) against the plain rule (a pass over the whole list, freed
+    slots zeroed, then the insertion): the same list words, count and overflow count, on 3,072 arenas x 80 ticks of
+    driving."""
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    libdir = os.path.join(ROOT, "rocketsim-cuda_b200")
+    if not os.path.exists(os.path.join(libdir, "librsx.so")):
+        pytest.skip("librsx.so is not built")
+    src = tmp_path / "cell_moves.cpp"
+    exe = tmp_path / "cell_moves"
+    src.write_text(P3A_PROGRAM)
+    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-I", CSRC, str(src), "-L", libdir, "-lrsx", f"-Wl,-rpath,{libdir}",
+           "-o", str(exe)]
+    cuda_lib = "/usr/local/cuda/lib64"
+    if os.path.isdir(cuda_lib):
+        cmd[-2:-2] = ["-L", cuda_lib, f"-Wl,-rpath,{cuda_lib}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    words = out.stdout.split()
+    assert int(words[words.index("moves") + 1]) > 1000, out.stdout
