@@ -287,6 +287,14 @@ RSX_F void cell_indices(const StaticData& D, V3 p, uint32_t out[3]) {
     out[a] = (uint32_t)m < hi ? (uint32_t)m : hi;
   }
 }
+// the index of the lowest set bit of x (x != 0)
+RSX_F int ctz64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+  return __ffsll((long long)x) - 1;
+#else
+  return __builtin_ctzll(x);
+#endif
+}
 RSX_F uint32_t cell_of(const StaticData& D, const uint32_t i[3]) { return i[0] * D.grid_n[1] * D.grid_n[2] + i[1] * D.grid_n[2] + i[2]; }
 // The first entry of the ray grid's dynamic list at or after cell c.  The list is sorted by cell (broad.cuh dyn_cells_block inserts
 // after every entry of a lower or equal cell and removes in place), so a cell's entries are one run from here, in list

@@ -415,7 +415,13 @@ RSX_F int pad_winner(const ArenaState& S, int p, float mx) {
 RSX_HD RSX_NOINL inline void pads_tick(ArenaState& S, const StaticData& D) {
   const float mx = D.mut[M_MAX_BOOST];
   int touching[kCars] = {-1, -1};
-  for (int i = 0; i < kPads; ++i) {
+  // the pads whose touching list is not empty (the loop below leaves an empty list as it is), read as independent loads
+  static_assert(kPads <= 64, "one bit per pad");
+  uint64_t listed_pads = 0;
+#pragma unroll
+  for (int i = 0; i < kPads; ++i) listed_pads |= (uint64_t)(S.pad_touch[i].n != 0) << i;
+  for (; listed_pads != 0; listed_pads &= listed_pads - 1) {
+    const int i = ctz64(listed_pads);
     const PadConst& pad = D.pads[i];
     PadTouch& t = S.pad_touch[i];
     uint32_t kept = 0;
