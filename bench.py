@@ -63,13 +63,13 @@ def _kc(rd, wr, inst, thr):
 
 
 KERNEL_COUNTERS = {
-    "k_sim8_multi": _kc(5121808640, 5043499008, 1544248756, 10639862898),
-    "k_sim8_lockstep_t448<7>": _kc(6275417344, 5839662848, 1561873949, 10961083412),
-    "k_sim8_lockstep_t512<7>": _kc(6254316544, 5820695296, 1562420893, 10977538140),
-    "k_sim8_lockstep_t448<14>": _kc(5897723392, 5585730304, 1216579710, 11677240224),
-    "k_sim8_lockstep_t512<14>": _kc(5923618816, 5604210176, 1220573075, 11758854438),
-    "k_sim8_lockstep_t448<15>": _kc(5877837312, 5572951040, 1178267483, 11955292729),
-    "k_sim8_lockstep_t512<15>": _kc(5912239104, 5595661056, 1181828751, 12060642031),
+    "k_sim8_multi": _kc(5126267136, 5056344576, 1534066674, 10436083984),
+    "k_sim8_lockstep_t448<7>": _kc(6258553856, 5842978816, 1551714381, 10758340571),
+    "k_sim8_lockstep_t512<7>": _kc(6255863552, 5833099776, 1552293325, 10775763619),
+    "k_sim8_lockstep_t448<14>": _kc(5870563840, 5579853312, 1213356967, 11506029617),
+    "k_sim8_lockstep_t512<14>": _kc(5894772480, 5602215168, 1217023574, 11597969422),
+    "k_sim8_lockstep_t448<15>": _kc(5848313600, 5567679232, 1167464173, 11751954768),
+    "k_sim8_lockstep_t512<15>": _kc(5877518848, 5585444608, 1172608364, 11849352609),
 }
 
 

@@ -190,11 +190,13 @@ class DecisionRunner:
                             "weights": [1.0] * P.LABELS})
         return out
 
-    def tune(self, controls_ptrs, candidates=None, repeats: int = 1):
+    def tune(self, controls_ptrs, candidates=None, repeats: int = 1, margin: float = 0.01):
         """Times every candidate on the same decisions from the same start states, `repeats` times each (the candidates
-        interleaved round by round, so that a slow stretch of the machine does not fall on one candidate); keeps the
-        fastest by median time as self.config (one lucky repeat does not decide; with one repeat the median is that
-        time).  Returns [(median ms, config, [ms of every repeat])] sorted by median time."""
+        interleaved round by round, so that a slow stretch of the machine does not fall on one candidate) and ranks
+        them by median time (one lucky repeat does not decide; with one repeat the median is that time).  Keeps as
+        self.config, among the candidates within `margin` of the best median, the one with the fewest kernel launches
+        per decision (a difference inside the run-to-run spread does not buy the predictor's extra launches).  Returns
+        [(median ms, config, [ms of every repeat])] sorted by median time."""
         t = self.torch
         snap = self.snapshot()
         cands = list(candidates or self.candidates())
@@ -212,7 +214,8 @@ class DecisionRunner:
         self.restore(snap)
         self.stream.synchronize()
         results = sorted(((sorted(ts)[(len(ts) - 1) // 2], c, ts) for ts, c in zip(times, cands)), key=lambda r: r[0])
-        self.config = dict(results[0][1])
+        close = [r for r in results if r[0] <= results[0][0] * (1.0 + margin)]
+        self.config = dict(min(close, key=lambda r: (self.kernels_per_step(r[1]), r[0]))[1])
         return results
 
     # ---- CUDA graphs ----
