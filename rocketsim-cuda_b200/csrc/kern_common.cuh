@@ -13,10 +13,11 @@ namespace {
 
 constexpr int kMaxBlock = 64;
 
+// (unrolled 32 deep: the copy is a chain of dependent-latency groups, one group of loads in flight at a time)
 __device__ __forceinline__ void load_tick(ArenaState* s, const uint32_t* buf, uint32_t a) {
   uint32_t* d = reinterpret_cast<uint32_t*>(s);
   const uint32_t* src = buf + (size_t)(a / kLanes) * aosoa_block_words() + (a % kLanes);
-#pragma unroll 8
+#pragma unroll 32
   for (int w = 0; w < kTickWords; ++w) d[w] = src[(size_t)w * kLanes];
 #pragma unroll 8
   for (int w = kTickWords; w < kArenaWords; ++w) d[w] = 0u;
@@ -24,7 +25,7 @@ __device__ __forceinline__ void load_tick(ArenaState* s, const uint32_t* buf, ui
 __device__ __forceinline__ void store_tick(uint32_t* buf, uint32_t a, const ArenaState* s) {
   const uint32_t* d = reinterpret_cast<const uint32_t*>(s);
   uint32_t* dst = buf + (size_t)(a / kLanes) * aosoa_block_words() + (a % kLanes);
-#pragma unroll 8
+#pragma unroll 32
   for (int w = 0; w < kTickWords; ++w) dst[(size_t)w * kLanes] = d[w];
 }
 
